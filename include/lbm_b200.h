@@ -1,0 +1,176 @@
+/*
+ * lbm_b200.h - C ABI of liblbm_b200.so, a B200 (sm_100a) D2Q9 lattice-Boltzmann
+ * collide-stream library that drops in for the kernels of Qianyv-Li8262/LBM-CUDA.
+ *
+ * Conventions shared by every entry point (they follow the reference kernels):
+ *   - populations are SoA float planes f[q*W*H + y*W + x], q in the order
+ *     c_x = {0,1,0,-1,0,1,-1,-1,1}, c_y = {0,0,1,0,-1,1,1,-1,-1} (lbm_core4.cu:1-3);
+ *   - the mask is one byte per cell, row-major y*W + x, nonzero = solid
+ *     (the reference passes a bool array, lbm_mine2.py:55-56);
+ *   - every pointer is device memory owned by the caller; apart from lbm_create,
+ *     no entry point allocates;
+ *   - work is enqueued on `stream` (a cudaStream_t; NULL = the legacy default stream)
+ *     and nothing synchronises, so calls can be captured into a CUDA graph as the
+ *     reference drivers do (lbm_mine2.py:75-81);
+ *   - the return value is 0 on success, the cudaError_t of a failing CUDA call
+ *     (1..999), or one of the LBM_ERR_* validation codes below.  The reference
+ *     kernels return nothing; their launch errors surface asynchronously.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_OK 0
+#define LBM_ERR_ARG 1001         /* null pointer, size or parameter out of range */
+#define LBM_ERR_UNSUPPORTED 1002 /* configuration not built (e.g. temporal depth T) */
+#define LBM_ERR_DEVICE 1003      /* no usable sm_100 device or driver entry point */
+#define LBM_ERR_TIMEOUT 1004     /* a bounded device-side wait gave up */
+
+/* Storage formats of the population planes (general solver). */
+#define LBM_STORE_F32 0
+#define LBM_STORE_F16DEV 1  /* IEEE half of f_q - w_q, FP32 arithmetic */
+#define LBM_STORE_BF16DEV 2 /* bfloat16 of f_q - w_q, FP32 arithmetic */
+
+/* Mask byte values of the general solver (the drop-ins treat nonzero as solid). */
+#define LBM_MASK_FLUID 0
+#define LBM_MASK_SOLID 1
+#define LBM_MASK_MOVING 2   /* wall moving with (u_lid, 0): Ladd bounce-back, rho_w = 1 */
+#define LBM_MASK_OBSTACLE 3 /* solid, included in the drag/lift momentum exchange */
+
+/* Domain sides of the general solver. */
+#define LBM_BC_WALL 0       /* stationary half-way bounce-back wall outside the domain */
+#define LBM_BC_PERIODIC 1   /* left: both x sides periodic; bc_y: both y sides periodic */
+#define LBM_BC_ZOUHE 2      /* left only: Zou-He velocity inlet, flat profile u_in */
+#define LBM_BC_ZOUHE_RAMP 3 /* left only: Zou-He with the reference's cosine ramp (lbm_core4.cu:46-51) */
+#define LBM_BC_OUTFLOW 4    /* right only: zero-gradient ghost column W-1 (lbm_core4.cu:114-116) */
+
+/* ------------------------------------------------------------------------
+ * Reference drop-ins.  Same argument order and meaning as the reference
+ * kernels, plus the stream and an int status.
+ * ------------------------------------------------------------------------ */
+
+/* One MRT + Smagorinsky pull step, f_now -> f_out, writing u, v, rho of every
+ * updated cell.  Replaces fused_lbmkernel of lbm_core4.cu:7-13 (launched at
+ * lbm_mine2.py:77-80).  Cs = 0.20 and s_e = s_eps = s_q = 1.1 as in the
+ * reference; tau_inv_bnd is accepted and unused, as in the reference (:12). */
+int lbm_core4_step(const uint8_t *mask, const float *f_now, float *f_out, float *ux, float *uy, float *rho, int W,
+                   int H, float tau_inv, float u_in, float tau_inv_bnd, void *stream);
+
+/* n_steps of lbm_core4_step in ping-pong order starting from f_a, fused T
+ * steps per launch (temporal blocking, 1 <= T <= 8).  The final state is in
+ * f_b when *result_in_b is set to 1, else in f_a.  u, v, rho are those of the
+ * last step.  Identical results to n_steps calls of lbm_core4_step when cells
+ * that are never updated (solid cells, rows 0 and H-1) are not fluid sources,
+ * which holds for the reference drivers' masks (lbm_mine2.py:49-53). */
+int lbm_core4_run(const uint8_t *mask, float *f_a, float *f_b, float *ux, float *uy, float *rho, int W, int H,
+                  float tau_inv, float u_in, int n_steps, int T, void *stream, int *result_in_b);
+
+/* T BGK steps (T even, 2..8) with the shared-memory AA pattern, f_now -> f_out,
+ * writing u, v, rho from the final canonical populations.  Replaces
+ * fused_lbmkernel of lbm_core_smemaa.cu:12-15 (T = 4 there, :8). */
+int lbm_smemaa_step(const uint8_t *mask, const float *f_now, float *f_out, float *ux, float *uy, float *rho, int W,
+                    int H, float tau_inv, float u_in, int T, void *stream);
+
+/* T BGK steps (T even, 2..8), first step read from f_now, last step scattered
+ * straight into f_out.  Replaces fused_lbmkernel of
+ * lbm_core_smemaa_policy.cu:78-80 and lbm_core_smemaa_endfused.cu:12-14
+ * (T = 6 there).  Entries of f_out that the final scatter does not reach keep
+ * their previous contents, as in the reference. */
+int lbm_blocked_step(const uint8_t *mask, const float *f_now, float *f_out, int W, int H, float tau_inv, float u_in,
+                     int T, void *stream);
+
+/* u, v, rho from canonical populations, Zou-He at x = 0.  Replaces macro_kernel
+ * of lbm_core_smemaa_policy.cu:431-433. */
+int lbm_macro(const float *f, float *ux, float *uy, float *rho, const uint8_t *mask, int W, int H, float u_in,
+              void *stream);
+
+/* Vorticity colour map into an RGBA8 device buffer (W*H*4 bytes).  Replaces
+ * visualizekernel of lbm_core4.cu:214-217; the buffer replaces the OpenGL
+ * pixel buffer of zero_copy_window.py:119-155. */
+int lbm_visualize(const float *ux, const float *uy, const float *rho, uint8_t *image, const uint8_t *mask, int W,
+                  int H, float vort_scale, void *stream);
+
+/* ------------------------------------------------------------------------
+ * General solver (no reference counterpart: the reference hard-codes these
+ * choices in its kernels, lbm_core4.cu:6,123).  Same SoA layout; the storage
+ * format selects 4-byte or 2-byte elements per population.
+ * ------------------------------------------------------------------------ */
+
+#define LBM_COLL_BGK 0
+#define LBM_COLL_MRT 1
+#define LBM_CLOSURE_NONE 0
+#define LBM_CLOSURE_SMAG 1
+
+typedef struct lbm_params {
+    int W, H;
+    int storage;   /* LBM_STORE_* */
+    int collision; /* LBM_COLL_* */
+    int closure;   /* LBM_CLOSURE_* */
+    float s_nu;    /* stress relaxation rate 1/tau, tau = 3 nu + 1/2 */
+    float s_e, s_eps, s_q; /* MRT rates of the energy, energy-square and heat-flux moments */
+    float cs_smag; /* Smagorinsky constant (LBM_CLOSURE_SMAG) */
+    int bc_left, bc_right, bc_y; /* LBM_BC_* */
+    float u_in;    /* Zou-He inlet velocity */
+    float u_lid;   /* x velocity of LBM_MASK_MOVING cells */
+    int ref_clamps; /* 1: the reference's stabilisers |u| <= 0.4, rho in [0,1.5], f in [0,10] */
+} lbm_params;
+
+typedef struct lbm_handle lbm_handle;
+
+/* Defaults: the lbm_core4.cu choices (MRT, s_e = s_eps = s_q = 1.1, Smagorinsky
+ * Cs = 0.2, Zou-He inlet with the ramp, outflow, walls in y, clamps on) with
+ * s_nu = 1.8 and u_in = 0.1 as in lbm_mine2.py:77-78. */
+void lbm_params_default(lbm_params *p, int W, int H);
+
+/* Validate the parameters and allocate the handle and its small reduction
+ * scratch (the only entry point that allocates); lbm_destroy frees them. */
+int lbm_create(const lbm_params *p, lbm_handle **out);
+int lbm_destroy(lbm_handle *h);
+
+/* Bytes of one population state (9 planes of W*H elements of the storage format). */
+size_t lbm_state_bytes(const lbm_handle *h);
+
+/* f := equilibrium of (rho, ux, uy) (device arrays of W*H floats; NULL = 1, 0, 0). */
+int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *ux, const float *uy, void *stream);
+
+/* n_steps pull steps in ping-pong order starting from f_a, fused T per launch
+ * (1 <= T <= 8).  The stored state is post-collision populations (the
+ * lbm_core4.cu convention).  u, v, rho of the last step are written when the
+ * pointers are non-NULL.  *result_in_b = 1 when the final state is in f_b. */
+int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_steps, int T, float *ux, float *uy,
+            float *rho, void *stream, int *result_in_b);
+
+/* Total mass and momentum sum_x sum_q f, c_x f, c_y f over cells with mask == 0,
+ * accumulated in FP64 with a fixed-order two-pass reduction (deterministic).
+ * d_out: 3 doubles of device memory. */
+int lbm_diag_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d_out, void *stream);
+
+/* Momentum-exchange force on LBM_MASK_OBSTACLE cells, sum 2 c_q f_q(x) over fluid
+ * x and directions q with x + c_q an obstacle cell, in FP64 (deterministic).
+ * d_out: 2 doubles (Fx = drag, Fy = lift) of device memory. */
+int lbm_forces_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d_out, void *stream);
+
+/* Convert a state between storage formats (W*H*9 elements each). */
+int lbm_convert_state(int W, int H, const void *src, int src_storage, void *dst, int dst_storage, void *stream);
+
+/* Read (and optionally clear) the device error word of the current device:
+ * bit 0 = a bounded device-side wait gave up.  Synchronises the device. */
+int lbm_device_error_flags(int *flags, int clear);
+
+/* Human-readable text for a status code (static storage). */
+const char *lbm_error_string(int status);
+
+/* Library version, major*10000 + minor*100 + patch. */
+int lbm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H */

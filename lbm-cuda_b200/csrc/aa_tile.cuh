@@ -1,0 +1,283 @@
+// Temporally blocked BGK with the AA pattern in shared memory: the drop-ins for
+// lbm_core_smemaa.cu (VARIANT_SMEMAA) and lbm_core_smemaa_policy.cu /
+// lbm_core_smemaa_endfused.cu (VARIANT_POLICY).
+//
+// The slot semantics are those of the reference, so its boundary behaviour is
+// reproduced exactly (the smem AA pattern, lbm_core_smemaa.cu:90-485):
+//   A phase  local collide, store reversed:    S[opp q](x) = f*_q(x)
+//   B phase  gather S[opp q](x - c_q) (or S[q](x) if x - c_q is solid),
+//            collide, scatter S[q](x + c_q) (or S[opp q](x) if x + c_q is
+//            solid; populations leaving x = 0 to the left are discarded)
+//   outlet   after each A (and, for smemaa, each B) column W-1 := column W-2
+// A cell is updated when it is in the domain, 0 < y < H-1, x < W-1 and not
+// solid; out-of-domain cells are solid with zero populations, column W-1 is
+// fluid (open outlet ghost).
+//
+// B200 design: one CTA of 256 threads owns a 64 x 32 tile (core (64-2T) x
+// (32-2T) plus a T-cell halo), fetched by a single TMA box [68 x 32 x 9] (plus
+// one for the mask) when the layout allows it.  Threads have a fixed 2-D map
+// (two warps per tile row, eight rows apart), so phases need no integer
+// division; per-cell neighbour codes are built once after the load, so the B
+// phase reads one 16-bit code instead of nine mask bytes.  Two CTAs fit per SM.
+#pragma once
+
+#include "collide.cuh"
+
+namespace lbm {
+
+enum : int { VARIANT_SMEMAA = 0, VARIANT_POLICY = 1 };
+
+struct AaParams {
+    const float *f_in;
+    float *f_out;
+    const uint8_t *mask;
+    float *ux, *uy, *rho; // VARIANT_SMEMAA only
+    int W, H;
+    int use_tma;
+    int *err;
+    Phys k;
+};
+
+template <int T_, int VAR_> struct AaCfg {
+    static constexpr int T = T_;
+    static constexpr int VAR = VAR_;
+    static constexpr int SX = 64, SY = 32; // tile incl. halo
+    static constexpr int CX = SX - 2 * T, CY = SY - 2 * T;
+    static constexpr int SW = SX + 4;      // smem row stride: room for the 16-byte TMA alignment offset
+    static constexpr int PL = SW * SY;     // floats per population plane
+    static constexpr int MW = SX + 16;     // mask row bytes (TMA box, 16-byte aligned origin)
+    static constexpr int NT = 256;
+    static constexpr int ROWS_PER_THREAD = SY / (NT / SX);
+    static constexpr int OFF_F = 128;
+    static constexpr int OFF_M = OFF_F + 9 * PL * 4;
+    static constexpr int OFF_C = OFF_M + round_up(MW * SY, 128);
+    static constexpr int SMEM = OFF_C + SX * SY * 2;
+    static constexpr uint32_t TX = 9 * PL * 4 + MW * SY;
+    static_assert(T % 2 == 0 && T >= 2 && CY > 0, "T");
+    static_assert(SMEM <= 113 * 1024, "two CTAs per SM");
+};
+
+// code bits: bit q (1..8) = the cell x - c_q is solid; bit 0 = cell updated.
+enum : uint16_t { AA_UPD = 1 };
+
+template <class C>
+__global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant__ AaParams p,
+                                                           const __grid_constant__ CUtensorMap tmf,
+                                                           const __grid_constant__ CUtensorMap tmm)
+{
+    constexpr int T = C::T, SX = C::SX, SY = C::SY, CX = C::CX, CY = C::CY, SW = C::SW, PL = C::PL, MW = C::MW;
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    float *S = reinterpret_cast<float *>(smem + C::OFF_F);
+    uint8_t *M = smem + C::OFF_M;
+    uint16_t *code = reinterpret_cast<uint16_t *>(smem + C::OFF_C);
+
+    const int W = p.W, H = p.H;
+    const int tid = threadIdx.x;
+    const int col = (tid & 31) + 32 * ((tid >> 5) & 1); // 0..63
+    const int rb = tid >> 6;                           // 0..3
+    const int xt = blockIdx.x * CX - T;                // global x of tile column 0
+    const int yt = blockIdx.y * CY - T;
+    const bool tma = p.use_tma != 0;
+    const int xf = tma ? floor_div(xt, 4) * 4 : xt; // global x of smem row entry 0
+    const int xm = tma ? floor_div(xt, 16) * 16 : xt;
+    const int of = xt - xf, om = xt - xm;
+
+    // ---- load the tile: canonical f (zero outside) and the mask ----
+    if (tma) {
+        if (tid == 0) {
+            mbar_init(bar, 1);
+            mbar_fence_init();
+            mbar_arrive_expect_tx(bar, C::TX);
+            tma_load_3d(S, &tmf, bar, xf, yt, 0);
+            tma_load_2d(M, &tmm, bar, xm, yt);
+        }
+        __syncthreads();
+        if (!mbar_wait_bounded(bar, 0)) {
+            if (p.err)
+                atomicOr(p.err, 1);
+            return; // every thread waits on the same barrier and gives up together
+        }
+    } else {
+        for (int e = tid; e < SX * SY; e += C::NT) {
+            const int c = e % SX, r = e / SX;
+            const int x = xt + c, y = yt + r;
+            const bool in = x >= 0 && x < W && y >= 0 && y < H;
+            const long long id = (long long)y * W + x;
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                S[q * PL + r * SW + c + of] = in ? p.f_in[q * (long long)W * H + id] : 0.0f;
+            M[r * MW + c + om] = in ? p.mask[id] : (uint8_t)0;
+        }
+        __syncthreads();
+    }
+
+    // ---- per-cell codes (solid test as lbm_core_smemaa.cu:39-70) ----
+    auto solid = [&](int c, int r) -> bool { // tile cell, may lie one cell outside the tile
+        const int x = xt + c, y = yt + r;
+        if (x < 0 || x >= W || y < 0 || y >= H)
+            return true;
+        if (x == W - 1)
+            return false;
+        if (c < 0 || c >= SX || r < 0 || r >= SY)
+            return true; // outside the tile: only read for cells whose results are discarded
+        return M[r * MW + c + om] != 0;
+    };
+#pragma unroll
+    for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
+        const int r = rb + 4 * j, c = col;
+        const int x = xt + c, y = yt + r;
+        uint16_t cd = 0;
+        if (x >= 0 && x < W - 1 && y > 0 && y < H - 1 && !solid(c, r))
+            cd |= AA_UPD;
+#pragma unroll
+        for (int q = 1; q < 9; ++q)
+            if (solid(c - cx(q), r - cy(q)))
+                cd |= (uint16_t)(1u << q);
+        code[r * SX + c] = cd;
+    }
+    __syncthreads();
+
+    auto sl = [&](int q, int c, int r) -> float & { return S[q * PL + r * SW + c + of]; };
+
+    const int cg = (W - 1) - xt; // tile column of the outlet ghost
+    const bool has_outlet = cg - 1 >= 0 && cg < SX;
+    auto ghost_copy = [&]() {
+        for (int e = tid; e < SY * 9; e += C::NT) {
+            const int r = e / 9, q = e % 9;
+            const int y = yt + r;
+            if (y >= 1 && y <= H - 2)
+                sl(q, cg, r) = sl(q, cg - 1, r);
+        }
+    };
+
+    auto bgk_cell = [&](float (&f)[9], int x, int y) {
+        float r, u, v;
+        collide<PhysBgkRef>(f, x == 0, y, p.k, r, u, v);
+    };
+
+    // A phase at margin m: local collide, reversed store.
+    auto phase_a = [&](int m) {
+#pragma unroll
+        for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
+            const int r = rb + 4 * j, c = col;
+            if (r < m || r >= SY - m || c < m || c >= SX - m)
+                continue;
+            if (!(code[r * SX + c] & AA_UPD))
+                continue;
+            float f[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                f[q] = sl(q, c, r);
+            bgk_cell(f, xt + c, yt + r);
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                sl(opp(q), c, r) = f[q];
+        }
+    };
+
+    // B phase at margin m: gather, collide, scatter (into smem, or for the
+    // policy variant's last stage straight into f_out).
+    auto phase_b = [&](int m, bool to_global) {
+#pragma unroll
+        for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
+            const int r = rb + 4 * j, c = col;
+            if (r < m || r >= SY - m || c < m || c >= SX - m)
+                continue;
+            const uint16_t cd = code[r * SX + c];
+            if (!(cd & AA_UPD))
+                continue;
+            const int x = xt + c, y = yt + r;
+            float f[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                f[q] = (cd & (1u << q)) ? sl(q, c, r) : sl(opp(q), c - cx(q), r - cy(q));
+            bgk_cell(f, x, y);
+            if (!to_global) {
+#pragma unroll
+                for (int q = 0; q < 9; ++q) {
+                    if (x == 0 && cx(q) < 0)
+                        sl(q, c + cx(q), r + cy(q)) = f[q]; // discard slot left of the inlet
+                    else if (q && (cd & (1u << opp(q))))  // x + c_q is solid: bounce back
+                        sl(opp(q), c, r) = f[q];
+                    else
+                        sl(q, c + cx(q), r + cy(q)) = f[q];
+                }
+            } else {
+                // B-final scatter, lbm_core_smemaa_policy.cu:387-421.
+                const long long N = (long long)W * H;
+#pragma unroll
+                for (int q = 0; q < 9; ++q) {
+                    if (x == 0 && cx(q) < 0)
+                        continue;
+                    int tx, ty, tq;
+                    if (q && (cd & (1u << opp(q)))) {
+                        tx = x;
+                        ty = y;
+                        tq = opp(q);
+                    } else {
+                        tx = x + cx(q);
+                        ty = y + cy(q);
+                        tq = q;
+                    }
+                    if (tx == W - 1)
+                        continue;
+                    if (tx < xt + T || tx >= xt + T + CX || ty < yt + T || ty >= yt + T + CY || tx < 0 || tx >= W ||
+                        ty < 0 || ty >= H)
+                        continue;
+                    float *dst = p.f_out + tq * N + (long long)ty * W + tx;
+                    dst[0] = f[q];
+                    if (tx == W - 2)
+                        dst[1] = f[q];
+                }
+            }
+        }
+    };
+
+    for (int pr = 0; pr < T / 2; ++pr) {
+        phase_a(2 * pr);
+        __syncthreads();
+        if (has_outlet) {
+            ghost_copy();
+            __syncthreads();
+        }
+        const bool last = pr == T / 2 - 1;
+        if (C::VAR == VARIANT_POLICY && last) {
+            phase_b(2 * pr + 1, true);
+            return;
+        }
+        phase_b(2 * pr + 1, false);
+        __syncthreads();
+        if (C::VAR == VARIANT_SMEMAA && has_outlet) {
+            ghost_copy();
+            __syncthreads();
+        }
+    }
+
+    // ---- smemaa epilogue: canonical core and u, v, rho (lbm_core_smemaa.cu:500-546) ----
+    const long long N = (long long)W * H;
+#pragma unroll
+    for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
+        const int r = rb + 4 * j, c = col;
+        if (r < T || r >= T + CY || c < T || c >= T + CX)
+            continue;
+        const int x = xt + c, y = yt + r;
+        if (x >= W || y >= H)
+            continue;
+        const long long id = (long long)y * W + x;
+        float f[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            f[q] = sl(q, c, r);
+            p.f_out[q * N + id] = f[q];
+        }
+        if (!solid(c, r) && x < W - 1 && y > 0 && y < H - 1) {
+            const float rr = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
+            p.ux[id] = ((f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7])) / rr;
+            p.uy[id] = ((f[2] - f[4]) + (f[5] + f[6]) - (f[7] + f[8])) / rr;
+            p.rho[id] = rr;
+        }
+    }
+}
+
+} // namespace lbm

@@ -1,0 +1,415 @@
+// C-ABI of the general solver: lbm_params / lbm_create / lbm_run, equilibrium
+// initialisation, FP64 diagnostics (mass, momentum, momentum-exchange forces)
+// and storage-format conversion.
+#include <stdlib.h>
+#include <string.h>
+
+#include "wave_launch.cuh"
+
+struct lbm_handle {
+    lbm_params p;
+    lbm::Phys k;
+    double *partials; // reduction scratch: kRedBlocks x 3 doubles
+};
+
+namespace lbm {
+
+constexpr int kRedBlocks = 296; // fixed, so that the FP64 reductions are deterministic
+constexpr int kRedThreads = 256;
+
+template <class St, int T, int NX> using GenCfg = WaveCfg<T, NX, PhysRuntime, St, MODE_GENERAL>;
+
+template <class St> static int general_launch(const WaveParams &p, int T, cudaStream_t s)
+{
+    switch (T) {
+    case 1:
+        return launch_wave<GenCfg<St, 1, 224>>(p, s);
+    case 2:
+        return launch_wave<GenCfg<St, 2, 128>>(p, s);
+    case 3:
+        return launch_wave<GenCfg<St, 3, 128>>(p, s);
+    case 4:
+        return launch_wave<GenCfg<St, 4, 128>>(p, s);
+    case 5:
+        return launch_wave<GenCfg<St, 5, 128>>(p, s);
+    case 6:
+        return launch_wave<GenCfg<St, 6, 128>>(p, s);
+    case 7:
+        return launch_wave<GenCfg<St, 7, 128>>(p, s);
+    case 8:
+        return launch_wave<GenCfg<St, 8, 128>>(p, s);
+    default:
+        return LBM_ERR_UNSUPPORTED;
+    }
+}
+
+static int elem_bytes(int storage)
+{
+    return storage == LBM_STORE_F32 ? 4 : 2;
+}
+
+template <class St> __device__ __forceinline__ float ld(const void *f, long long i, int q)
+{
+    return St::load(reinterpret_cast<const typename St::T *>(f)[i], q);
+}
+
+template <class St>
+__global__ void equilibrium_kernel(void *f, const float *rho, const float *ux, const float *uy, long long N)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
+        const float r = rho ? rho[i] : 1.0f;
+        const float u = ux ? ux[i] : 0.0f;
+        const float v = uy ? uy[i] : 0.0f;
+        const float usq = u * u + v * v;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const float cu = (float)cx(q) * u + (float)cy(q) * v;
+            const float feq = wgt(q) * r * (1.0f + 3.0f * cu + 4.5f * cu * cu - 1.5f * usq);
+            reinterpret_cast<typename St::T *>(f)[q * N + i] = St::store(feq, q);
+        }
+    }
+}
+
+template <class Si, class So> __global__ void convert_kernel(const void *src, void *dst, long long n9, long long N)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n9; i += (long long)gridDim.x * blockDim.x) {
+        const int q = (int)(i / N);
+        const float v = Si::load(reinterpret_cast<const typename Si::T *>(src)[i], q);
+        reinterpret_cast<typename So::T *>(dst)[i] = So::store(v, q);
+    }
+}
+
+// Fixed-shape block reduction of NV doubles (same order on every run).
+template <int NV> __device__ void block_reduce(double (&v)[NV], double *out)
+{
+    __shared__ double red[kRedThreads / 32][NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < NV; ++c)
+        for (int o = 16; o > 0; o >>= 1)
+            v[c] += __shfl_down_sync(0xffffffffu, v[c], o);
+    if (lane == 0)
+#pragma unroll
+        for (int c = 0; c < NV; ++c)
+            red[warp][c] = v[c];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int c = 0; c < NV; ++c) {
+            double s = 0.0;
+            for (int w = 0; w < kRedThreads / 32; ++w)
+                s += red[w][c];
+            out[c] = s;
+        }
+    }
+}
+
+template <class St>
+__global__ void __launch_bounds__(kRedThreads) diag_partial_kernel(const void *f, const uint8_t *mask, long long N,
+                                                                    double *part)
+{
+    double v[3] = {0.0, 0.0, 0.0};
+    for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < N; i += (long long)gridDim.x * kRedThreads) {
+        if (mask[i])
+            continue;
+        float fl[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+            fl[q] = ld<St>(f, q * N + i, q);
+        double m = 0.0, jx = 0.0, jy = 0.0;
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            m += (double)fl[q];
+            jx += (double)(cx(q) * fl[q]);
+            jy += (double)(cy(q) * fl[q]);
+        }
+        v[0] += m;
+        v[1] += jx;
+        v[2] += jy;
+    }
+    block_reduce<3>(v, part + 3 * blockIdx.x);
+}
+
+template <class St>
+__global__ void __launch_bounds__(kRedThreads) forces_partial_kernel(const void *f, const uint8_t *mask, int W, int H,
+                                                                      double *part)
+{
+    const long long N = (long long)W * H;
+    double v[2] = {0.0, 0.0};
+    for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < N; i += (long long)gridDim.x * kRedThreads) {
+        if (mask[i])
+            continue;
+        const int x = (int)(i % W), y = (int)(i / W);
+#pragma unroll
+        for (int q = 1; q < 9; ++q) {
+            const int nx = x + cx(q), ny = y + cy(q);
+            if (nx < 0 || nx >= W || ny < 0 || ny >= H)
+                continue;
+            if (mask[(long long)ny * W + nx] != LBM_MASK_OBSTACLE)
+                continue;
+            const double fq = (double)ld<St>(f, q * N + i, q);
+            v[0] += 2.0 * cx(q) * fq;
+            v[1] += 2.0 * cy(q) * fq;
+        }
+    }
+    block_reduce<2>(v, part + 3 * blockIdx.x);
+}
+
+template <int NV> __global__ void __launch_bounds__(kRedThreads) final_reduce_kernel(const double *part, int n, double *out)
+{
+    double v[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c)
+        v[c] = 0.0;
+    for (int b = threadIdx.x; b < n; b += kRedThreads)
+#pragma unroll
+        for (int c = 0; c < NV; ++c)
+            v[c] += part[3 * b + c];
+    block_reduce<NV>(v, out);
+}
+
+template <class F> static int by_storage(int storage, F &&fn)
+{
+    switch (storage) {
+    case LBM_STORE_F32:
+        return fn(StoreF32{});
+    case LBM_STORE_F16DEV:
+        return fn(StoreF16Dev{});
+    case LBM_STORE_BF16DEV:
+        return fn(StoreBF16Dev{});
+    default:
+        return LBM_ERR_ARG;
+    }
+}
+
+static int validate(const lbm_params *p)
+{
+    if (!p || p->W < 3 || p->H < 3)
+        return LBM_ERR_ARG;
+    if ((long long)p->W * p->H * 9 > (1ll << 40))
+        return LBM_ERR_ARG;
+    if (p->storage < LBM_STORE_F32 || p->storage > LBM_STORE_BF16DEV)
+        return LBM_ERR_ARG;
+    if (p->collision != LBM_COLL_BGK && p->collision != LBM_COLL_MRT)
+        return LBM_ERR_ARG;
+    if (p->closure != LBM_CLOSURE_NONE && p->closure != LBM_CLOSURE_SMAG)
+        return LBM_ERR_UNSUPPORTED;
+    if (!(p->s_nu > 0.0f && p->s_nu < 2.0f))
+        return LBM_ERR_ARG;
+    const int l = p->bc_left, r = p->bc_right, y = p->bc_y;
+    if (l != LBM_BC_WALL && l != LBM_BC_PERIODIC && l != LBM_BC_ZOUHE && l != LBM_BC_ZOUHE_RAMP)
+        return LBM_ERR_ARG;
+    if (r != LBM_BC_WALL && r != LBM_BC_PERIODIC && r != LBM_BC_OUTFLOW)
+        return LBM_ERR_ARG;
+    if ((l == LBM_BC_PERIODIC) != (r == LBM_BC_PERIODIC))
+        return LBM_ERR_ARG;
+    if (y != LBM_BC_WALL && y != LBM_BC_PERIODIC)
+        return LBM_ERR_ARG;
+    return LBM_OK;
+}
+
+static Phys make_phys(const lbm_params &p)
+{
+    Phys k;
+    memset(&k, 0, sizeof(k));
+    k.s_nu = p.s_nu;
+    k.s_e = p.s_e;
+    k.s_eps = p.s_eps;
+    k.s_q = p.s_q;
+    k.tau0 = 1.0f / p.s_nu;
+    k.cs2x18 = 18.0f * p.cs_smag * p.cs_smag;
+    k.u_in = p.u_in;
+    k.u_lid = p.u_lid;
+    k.H = p.H;
+    k.ramp = p.bc_left == LBM_BC_ZOUHE_RAMP;
+    k.flags = (p.collision == LBM_COLL_MRT ? PF_MRT : 0) | (p.closure == LBM_CLOSURE_SMAG ? PF_SMAG : 0) |
+              (p.ref_clamps ? (PF_CLAMPU | PF_CLAMPF) : 0);
+    return k;
+}
+
+static int grid_for(long long n)
+{
+    long long g = (n + 255) / 256;
+    const long long cap = 16ll * sm_count();
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+} // namespace lbm
+
+using namespace lbm;
+
+extern "C" {
+
+void lbm_params_default(lbm_params *p, int W, int H)
+{
+    if (!p)
+        return;
+    memset(p, 0, sizeof(*p));
+    p->W = W;
+    p->H = H;
+    p->storage = LBM_STORE_F32;
+    p->collision = LBM_COLL_MRT;
+    p->closure = LBM_CLOSURE_SMAG;
+    p->s_nu = 1.8f;
+    p->s_e = p->s_eps = p->s_q = 1.1f;
+    p->cs_smag = 0.2f;
+    p->bc_left = LBM_BC_ZOUHE_RAMP;
+    p->bc_right = LBM_BC_OUTFLOW;
+    p->bc_y = LBM_BC_WALL;
+    p->u_in = 0.1f;
+    p->u_lid = 0.0f;
+    p->ref_clamps = 1;
+}
+
+int lbm_create(const lbm_params *p, lbm_handle **out)
+{
+    if (!out)
+        return LBM_ERR_ARG;
+    *out = nullptr;
+    int rc = validate(p);
+    if (rc)
+        return rc;
+    lbm_handle *h = static_cast<lbm_handle *>(calloc(1, sizeof(lbm_handle)));
+    if (!h)
+        return LBM_ERR_ARG;
+    h->p = *p;
+    h->k = make_phys(*p);
+    cudaError_t e = cudaMalloc(&h->partials, sizeof(double) * 3 * kRedBlocks);
+    if (e != cudaSuccess) {
+        free(h);
+        return status(e);
+    }
+    *out = h;
+    return LBM_OK;
+}
+
+int lbm_destroy(lbm_handle *h)
+{
+    if (!h)
+        return LBM_ERR_ARG;
+    cudaError_t e = cudaFree(h->partials);
+    free(h);
+    return status(e);
+}
+
+size_t lbm_state_bytes(const lbm_handle *h)
+{
+    return h ? (size_t)h->p.W * h->p.H * 9 * elem_bytes(h->p.storage) : 0;
+}
+
+int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *ux, const float *uy, void *stream)
+{
+    if (!h || !f)
+        return LBM_ERR_ARG;
+    const long long N = (long long)h->p.W * h->p.H;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return by_storage(h->p.storage, [&](auto st) {
+        using St = decltype(st);
+        equilibrium_kernel<St><<<grid_for(N), 256, 0, s>>>(f, rho, ux, uy, N);
+        return status(cudaGetLastError());
+    });
+}
+
+int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_steps, int T, float *ux, float *uy,
+            float *rho, void *stream, int *result_in_b)
+{
+    if (!h || !f_a || !f_b || !mask || f_a == f_b || n_steps < 0 || T < 1 || T > 8)
+        return LBM_ERR_ARG;
+    if ((ux || uy || rho) && !(ux && uy && rho))
+        return LBM_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    void *src = f_a, *dst = f_b;
+    int launches = 0;
+    for (int done = 0; done < n_steps;) {
+        const int t = (n_steps - done < T) ? (n_steps - done) : T;
+        const bool last = done + t == n_steps;
+        WaveParams wp;
+        memset(&wp, 0, sizeof(wp));
+        wp.f_in = src;
+        wp.f_out = dst;
+        wp.mask = mask;
+        if (last) {
+            wp.ux = ux;
+            wp.uy = uy;
+            wp.rho = rho;
+        }
+        wp.W = h->p.W;
+        wp.H = h->p.H;
+        wp.pitch = h->p.W;
+        wp.plane = (long long)h->p.W * h->p.H;
+        wp.mask_pitch = h->p.W;
+        wp.chunk = 0;
+        wp.bc_left = h->p.bc_left;
+        wp.bc_right = h->p.bc_right;
+        wp.bc_y = h->p.bc_y;
+        wp.use_tma = 1;
+        wp.k = h->k;
+        int rc = by_storage(h->p.storage, [&](auto st) { return general_launch<decltype(st)>(wp, t, s); });
+        if (rc)
+            return rc;
+        done += t;
+        ++launches;
+        void *tmp = src;
+        src = dst;
+        dst = tmp;
+    }
+    if (result_in_b)
+        *result_in_b = launches & 1;
+    return LBM_OK;
+}
+
+int lbm_diag_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d_out, void *stream)
+{
+    if (!h || !f || !mask || !d_out)
+        return LBM_ERR_ARG;
+    const long long N = (long long)h->p.W * h->p.H;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return by_storage(h->p.storage, [&](auto st) {
+        using St = decltype(st);
+        diag_partial_kernel<St><<<kRedBlocks, kRedThreads, 0, s>>>(f, mask, N, h->partials);
+        final_reduce_kernel<3><<<1, kRedThreads, 0, s>>>(h->partials, kRedBlocks, d_out);
+        return status(cudaGetLastError());
+    });
+}
+
+int lbm_forces_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d_out, void *stream)
+{
+    if (!h || !f || !mask || !d_out)
+        return LBM_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return by_storage(h->p.storage, [&](auto st) {
+        using St = decltype(st);
+        forces_partial_kernel<St><<<kRedBlocks, kRedThreads, 0, s>>>(f, mask, h->p.W, h->p.H, h->partials);
+        final_reduce_kernel<2><<<1, kRedThreads, 0, s>>>(h->partials, kRedBlocks, d_out);
+        return status(cudaGetLastError());
+    });
+}
+
+int lbm_convert_state(int W, int H, const void *src, int src_storage, void *dst, int dst_storage, void *stream)
+{
+    if (!src || !dst || W < 1 || H < 1 || src == dst)
+        return LBM_ERR_ARG;
+    const long long N = (long long)W * H;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return by_storage(src_storage, [&](auto si) {
+        return by_storage(dst_storage, [&](auto so) {
+            convert_kernel<decltype(si), decltype(so)><<<grid_for(9 * N), 256, 0, s>>>(src, dst, 9 * N, N);
+            return status(cudaGetLastError());
+        });
+    });
+}
+
+int lbm_device_error_flags(int *flags, int clear)
+{
+    if (!flags)
+        return LBM_ERR_ARG;
+    int *w = device_error_word();
+    if (!w)
+        return LBM_ERR_DEVICE;
+    cudaError_t e = cudaMemcpy(flags, w, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && clear)
+        e = cudaMemset(w, 0, sizeof(int));
+    return status(e);
+}
+
+} // extern "C"

@@ -1,0 +1,184 @@
+// Per-cell D2Q9 physics: Zou-He inlet, moments, Smagorinsky, MRT and BGK relaxation.
+//
+// The arithmetic follows the reference kernels (the library is compiled with
+// -use_fast_math, as the reference drivers compile theirs, lbm_mine2.py:69):
+//   Zou-He with the cosine ramp      lbm_core4.cu:46-57
+//   moments, clamps                  lbm_core4.cu:129-144
+//   Smagorinsky tau_eff              lbm_core4.cu:171-177
+//   MRT relax + inverse transform    lbm_core4.cu:150-199
+//   BGK                              lbm_core_smemaa.cu:206-212
+#pragma once
+
+#include "common.cuh"
+
+namespace lbm {
+
+// Runtime constants of one launch.
+struct Phys {
+    float s_nu;   // stress relaxation rate 1/tau (tau_inv of the reference)
+    float s_e;    // energy
+    float s_eps;  // energy square
+    float s_q;    // heat flux
+    float tau0;   // 1 / s_nu
+    float cs2x18; // 18 Cs^2 (Smagorinsky)
+    float u_in;   // inlet velocity
+    float u_lid;  // moving-wall x velocity (Ladd)
+    int H;        // domain height (ramp profile)
+    int ramp;     // 1: cosine-ramped inlet profile (reference), 0: flat
+    int flags;    // PF_* (used by PhysRuntime only)
+};
+
+enum : int { PF_MRT = 1, PF_SMAG = 2, PF_CLAMPU = 4, PF_CLAMPF = 8, PF_INLET_SMAG = 16 };
+
+// Compile-time physics variant.
+//   kMrt       MRT (else BGK)
+//   kSmag      Smagorinsky-corrected stress rate in the interior
+//   kClampU    the reference's velocity/density clamps |u| <= 0.4, rho in [0, 1.5]
+//              (lbm_core4.cu:142-144)
+//   kClampF    the reference's population clamp f in [0, 10] (lbm_core4.cu:203,
+//              lbm_core_smemaa.cu:220)
+//   kInletSmag Smagorinsky also at the Zou-He inlet (the reference does not)
+template <bool kMrt_, bool kSmag_, bool kClampU_, bool kClampF_, bool kInletSmag_> struct Physics {
+    static constexpr bool kRuntime = false;
+    static constexpr bool kMrt = kMrt_;
+    static constexpr bool kSmag = kSmag_;
+    static constexpr bool kClampU = kClampU_;
+    static constexpr bool kClampF = kClampF_;
+    static constexpr bool kInletSmag = kInletSmag_;
+};
+
+// lbm_core4.cu semantics: MRT + Smagorinsky, clamps, plain MRT at the inlet.
+using PhysCore4 = Physics<true, true, true, true, false>;
+// lbm_core_smemaa*.cu semantics: BGK, population clamp only.
+using PhysBgkRef = Physics<false, false, false, true, false>;
+// General solver: the same choices read from Phys::flags (uniform branches).
+struct PhysRuntime {
+    static constexpr bool kRuntime = true;
+    static constexpr bool kMrt = true, kSmag = true, kClampU = true, kClampF = true, kInletSmag = true;
+};
+
+__device__ __forceinline__ float inlet_u(const Phys &k, int y)
+{
+    if (!k.ramp)
+        return k.u_in;
+    float d = fminf((float)y, (float)(k.H - 1 - y));
+    float sm = 1.0f;
+    if (d < 50.0f)
+        sm = 0.5f * (1.0f - cosf(3.14159f * d / 50.0f));
+    return k.u_in * sm;
+}
+
+// Zou-He velocity inlet: overwrites f1, f5, f8 and returns rho (lbm_core4.cu:54-57).
+__device__ __forceinline__ float zou_he(float (&f)[9], float lu)
+{
+    float rho = (f[0] + f[2] + f[4] + 2.0f * (f[3] + f[6] + f[7])) / (1.0f - lu);
+    float a = 0.16666666666f * rho * lu;
+    float h = 0.5f * (f[2] - f[4]);
+    f[1] = f[3] + 0.666666667f * rho * lu;
+    f[5] = f[7] - h + a;
+    f[8] = f[6] + h + a;
+    return rho;
+}
+
+// Smagorinsky stress relaxation rate from the non-equilibrium stress moments.
+__device__ __forceinline__ float smag_rate(const float (&f)[9], float r, float u, float v, const Phys &k)
+{
+    float n7 = (f[1] - f[2] + f[3] - f[4]) - r * (u * u - v * v);
+    float n8 = (f[5] - f[6] + f[7] - f[8]) - r * u * v;
+    float Q = sqrtf(n7 * n7 + n8 * n8 + 1e-8f);
+    float tau_eff = 0.5f * (k.tau0 + sqrtf(k.tau0 * k.tau0 + k.cs2x18 * Q / r));
+    return 1.0f / tau_eff;
+}
+
+// MRT relaxation in the Lallemand-Luo basis and inverse transform.  m0 = r,
+// m3 = r u and m5 = r v are the values chosen by the caller.
+__device__ __forceinline__ void mrt_relax(float (&f)[9], float r, float u, float v, float s_e, float s_eps, float s_q,
+                                          float s_nu)
+{
+    const float f14 = f[1] + f[2] + f[3] + f[4];
+    const float f58 = f[5] + f[6] + f[7] + f[8];
+    float m1 = -4.0f * f[0] + 2.0f * f58 - f14;
+    float m2 = 4.0f * f[0] + f58 - 2.0f * f14;
+    const float m3 = r * u;
+    float m4 = -2.0f * (f[1] - f[3]) + f[5] - f[6] - f[7] + f[8];
+    const float m5 = r * v;
+    float m6 = -2.0f * (f[2] - f[4]) + f[5] + f[6] - f[7] - f[8];
+    float m7 = f[1] - f[2] + f[3] - f[4];
+    float m8 = f[5] - f[6] + f[7] - f[8];
+    const float usq = u * u + v * v;
+    m1 -= s_e * (m1 - (3.0f * usq - 2.0f) * r);
+    m2 -= s_eps * (m2 - (1.0f - 3.0f * usq) * r);
+    m4 -= s_q * (m4 + m3);
+    m6 -= s_q * (m6 + m5);
+    m7 -= s_nu * (m7 - r * (u * u - v * v));
+    m8 -= s_nu * (m8 - r * u * v);
+    const float inv9 = 0.1111111111f, inv36 = 0.02777777778f;
+    const float t0 = r - m1 + m2;
+    const float t1 = 4.0f * r - m1 - 2.0f * m2;
+    const float t2 = 4.0f * r + 2.0f * m1 + m2;
+    f[0] = t0 * inv9;
+    f[1] = (t1 + 6.0f * m3 - 6.0f * m4 + 9.0f * m7) * inv36;
+    f[2] = (t1 + 6.0f * m5 - 6.0f * m6 - 9.0f * m7) * inv36;
+    f[3] = (t1 - 6.0f * m3 + 6.0f * m4 + 9.0f * m7) * inv36;
+    f[4] = (t1 - 6.0f * m5 + 6.0f * m6 - 9.0f * m7) * inv36;
+    f[5] = (t2 + 6.0f * m3 + 3.0f * m4 + 6.0f * m5 + 3.0f * m6 + 9.0f * m8) * inv36;
+    f[6] = (t2 - 6.0f * m3 - 3.0f * m4 + 6.0f * m5 + 3.0f * m6 - 9.0f * m8) * inv36;
+    f[7] = (t2 - 6.0f * m3 - 3.0f * m4 - 6.0f * m5 - 3.0f * m6 + 9.0f * m8) * inv36;
+    f[8] = (t2 + 6.0f * m3 + 3.0f * m4 - 6.0f * m5 - 3.0f * m6 - 9.0f * m8) * inv36;
+}
+
+__device__ __forceinline__ void bgk_relax(float (&f)[9], float r, float u, float v, float s_nu)
+{
+    const float usq = u * u + v * v;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        float cu = (float)cx(q) * u + (float)cy(q) * v;
+        float feq = wgt(q) * r * (1.0f + 3.0f * cu + 4.5f * cu * cu - 1.5f * usq);
+        f[q] += s_nu * (feq - f[q]);
+    }
+}
+
+// Full collision of one updated cell.  `inlet` selects the Zou-He branch
+// (x = 0, prescribed velocity); r/u/v receive the macroscopic values the
+// reference writes to its rho/ux/uy arrays.
+template <class Ph>
+__device__ __forceinline__ void collide(float (&f)[9], bool inlet, int y, const Phys &k, float &r, float &u, float &v)
+{
+    const bool kMrt = Ph::kRuntime ? (k.flags & PF_MRT) != 0 : Ph::kMrt;
+    const bool kSmag = Ph::kRuntime ? (k.flags & PF_SMAG) != 0 : Ph::kSmag;
+    const bool kClampU = Ph::kRuntime ? (k.flags & PF_CLAMPU) != 0 : Ph::kClampU;
+    const bool kClampF = Ph::kRuntime ? (k.flags & PF_CLAMPF) != 0 : Ph::kClampF;
+    const bool kInletSmag = Ph::kRuntime ? (k.flags & PF_INLET_SMAG) != 0 : Ph::kInletSmag;
+    r = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
+    const float jx = (f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7]);
+    const float jy = (f[2] - f[4]) + (f[5] + f[6]) - (f[7] + f[8]);
+    u = jx / r;
+    v = jy / r;
+    if (kClampU) {
+        u = fminf(0.4f, fmaxf(-0.4f, u));
+        v = fminf(0.4f, fmaxf(-0.4f, v));
+        r = fminf(1.5f, fmaxf(0.0f, r));
+    }
+    if (inlet) {
+        const float lu = inlet_u(k, y);
+        r = zou_he(f, lu);
+        u = lu;
+        v = 0.0f;
+    }
+    float s = k.s_nu;
+    if (kSmag) {
+        if (kInletSmag || !inlet)
+            s = smag_rate(f, r, u, v, k);
+    }
+    if (kMrt)
+        mrt_relax(f, r, u, v, k.s_e, k.s_eps, k.s_q, s);
+    else
+        bgk_relax(f, r, u, v, s);
+    if (kClampF) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+            f[q] = fminf(10.0f, fmaxf(0.0f, f[q]));
+    }
+}
+
+} // namespace lbm

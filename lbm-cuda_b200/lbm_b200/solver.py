@@ -1,0 +1,128 @@
+"""General solver (lbm_params / lbm_create / lbm_run) with torch device arrays."""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _lib
+from ._lib import call, lib
+
+STORE_F32, STORE_F16DEV, STORE_BF16DEV = 0, 1, 2
+COLL_BGK, COLL_MRT = 0, 1
+CLOSURE_NONE, CLOSURE_SMAG = 0, 1
+BC_WALL, BC_PERIODIC, BC_ZOUHE, BC_ZOUHE_RAMP, BC_OUTFLOW = 0, 1, 2, 3, 4
+
+
+class Params(C.Structure):
+    """Mirror of ``lbm_params`` (include/lbm_b200.h)."""
+
+    _fields_ = [
+        ("W", C.c_int), ("H", C.c_int), ("storage", C.c_int), ("collision", C.c_int), ("closure", C.c_int),
+        ("s_nu", C.c_float), ("s_e", C.c_float), ("s_eps", C.c_float), ("s_q", C.c_float),
+        ("cs_smag", C.c_float), ("bc_left", C.c_int), ("bc_right", C.c_int), ("bc_y", C.c_int),
+        ("u_in", C.c_float), ("u_lid", C.c_float), ("ref_clamps", C.c_int),
+    ]
+
+
+def default_params(W: int, H: int, **overrides) -> Params:
+    p = Params()
+    lib().lbm_params_default(C.byref(p), int(W), int(H))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(f"lbm_params has no field {k!r}")
+        setattr(p, k, v)
+    return p
+
+
+def _torch_dtype(storage: int):
+    import torch
+
+    return {STORE_F32: torch.float32, STORE_F16DEV: torch.float16, STORE_BF16DEV: torch.bfloat16}[storage]
+
+
+class Solver:
+    """Owns an lbm_handle.  States are torch tensors shaped (9, H, W) in the
+    handle's storage format (float32, or float16/bfloat16 holding f_q - w_q)."""
+
+    def __init__(self, W: int, H: int, params: Params | None = None, **overrides):
+        self.params = params if params is not None else default_params(W, H, **overrides)
+        self.W, self.H = int(self.params.W), int(self.params.H)
+        h = C.c_void_p(0)
+        call("lbm_create", C.byref(self.params), C.byref(h))
+        self._h = h
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise RuntimeError("solver is closed")
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            call("lbm_destroy", self._h)
+            self._h = C.c_void_p(0)
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def dtype(self):
+        return _torch_dtype(self.params.storage)
+
+    def new_state(self):
+        import torch
+
+        return torch.empty((9, self.H, self.W), dtype=self.dtype, device="cuda")
+
+    def init_equilibrium(self, f, rho=None, ux=None, uy=None, stream=None):
+        from . import _ptr, _stream
+
+        call("lbm_init_equilibrium", self.handle, _ptr(f), _ptr(rho), _ptr(ux), _ptr(uy), _stream(stream))
+
+    def run(self, f_a, f_b, mask, n_steps: int, T: int = 4, ux=None, uy=None, rho=None, stream=None) -> int:
+        """n_steps steps fused T per launch; returns 1 when the result is in f_b."""
+        from . import _ptr, _stream
+
+        out = C.c_int(0)
+        call("lbm_run", self.handle, _ptr(f_a), _ptr(f_b), _ptr(mask), int(n_steps), int(T), _ptr(ux), _ptr(uy),
+             _ptr(rho), _stream(stream), C.byref(out))
+        return out.value
+
+    def diag(self, f, mask, out=None, stream=None):
+        """Device tensor [mass, momentum_x, momentum_y] (float64), fixed-order reduction."""
+        import torch
+
+        from . import _ptr, _stream
+
+        out = torch.empty(3, dtype=torch.float64, device="cuda") if out is None else out
+        call("lbm_diag_fp64", self.handle, _ptr(f), _ptr(mask), _ptr(out), _stream(stream))
+        return out
+
+    def forces(self, f, mask, out=None, stream=None):
+        """Device tensor [drag, lift] (float64), momentum exchange on LBM_MASK_OBSTACLE cells."""
+        import torch
+
+        from . import _ptr, _stream
+
+        out = torch.empty(2, dtype=torch.float64, device="cuda") if out is None else out
+        call("lbm_forces_fp64", self.handle, _ptr(f), _ptr(mask), _ptr(out), _stream(stream))
+        return out
+
+
+def convert_state(src, src_storage: int, dst, dst_storage: int, stream=None) -> None:
+    from . import _ptr, _stream
+
+    _, H, W = src.shape
+    call("lbm_convert_state", int(W), int(H), _ptr(src), int(src_storage), _ptr(dst), int(dst_storage),
+         _stream(stream))
+
+
+def device_error_flags(clear: bool = True) -> int:
+    v = C.c_int(0)
+    call("lbm_device_error_flags", C.byref(v), int(bool(clear)))
+    return v.value
+
+
+__all__ = ["Params", "Solver", "default_params", "convert_state", "device_error_flags", "_lib"]
