@@ -1,0 +1,365 @@
+#!/usr/bin/env python3
+"""Benchmark of the D2Q9 collide-stream hot path (one JSON line on rank 0).
+
+Workload (the channel-flow-past-a-cylinder configuration): 4096 x 1024 D2Q9,
+MRT + Smagorinsky (Cs = 0.1), FP32, Zou-He velocity inlet u = 0.05 (cosine
+ramp as in the reference), zero-gradient outlet, bounce-back channel walls,
+cylinder D = 128 centred at (1024, 512), nu = 6.4e-4 (tau = 0.50192),
+initial u_y noise uniform +-1e-4 from numpy PCG64 seed 0, T = 4 steps fused
+per launch.  Synthetic inputs with that shape (there is no external dataset).
+
+One bench "step" is one frame of `--frame` physical steps (default 100 =
+25 launches of T = 4).  Metric: MLUPS = W*H*physical steps / time, counting
+every cell as the reference does (lbm_mine2.py:106).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the reference's own kernel for this path
+(fused_lbmkernel of lbm_core4.cu, MRT + Smagorinsky, one step per launch,
+compiled from its source into oracle/_ref/) on the same workload.  Under
+torchrun every rank runs an independent replica (weak scaling, no data-path
+collective); the reference arm runs on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "lbm-cuda_b200"))
+
+W, H = 4096, 1024
+CYL = (1024, 512, 128)
+NU = 6.4e-4
+TAU = 3.0 * NU + 0.5
+U_IN = 0.05
+CS = 0.1
+B_ALG = 72.0  # algorithmic bytes per lattice update, FP32: one read + one write of 9 populations
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+HBM_FALLBACK_GBS = 6650.0
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+def workload():
+    from lbm_b200 import init as I
+
+    mask = I.cylinder_mask(W, H, CYL[0], CYL[1], CYL[2], value=I.OBSTACLE)
+    f0 = I.channel_state(W, H, u0=0.0, noise=1e-4, seed=0)
+    return mask, f0
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(seconds: float = 12.0):
+    """The oracle's OpenMP FP32 port of the per-cell update (lbm_core4.cu:120-211
+    with this workload's Cs and rates) on every host core, time-bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    lib = O.lib(cpu_baseline=True)
+    cores = int(lib.orc_num_threads())
+    mask, f0 = workload()
+    a, b = f0.copy(), f0.copy()
+    mac = tuple(np.zeros((H, W), np.float32) for _ in range(3))
+    O.core4_step(mask, a, b, mac, tau_inv=1.0 / TAU, u_in=U_IN, cs=CS, cpu_baseline=True)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        O.core4_step(mask, a, b, mac, tau_inv=1.0 / TAU, u_in=U_IN, cs=CS, cpu_baseline=True)
+        a, b = b, a
+        n += 1
+        dt = time.perf_counter() - t0
+        if (dt >= seconds and n >= 5) or n >= 2000:
+            break
+    return {"value": round(W * H * n / dt / 1e6, 2), "unit": "MLUPS", "cores": cores, "kind": "port",
+            "sample": f"{n} steps of the full {W}x{H} workload ({dt:.1f} s, FP32, OpenMP)"}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--T", type=int, default=4, help="steps fused per launch (ours)")
+    ap.add_argument("--frame", type=int, default=100, help="physical steps per bench step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank, world, local = dist_env()
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    if args.impl == "reference":
+        if rank != 0:
+            barrier()
+            if world > 1:
+                dist.destroy_process_group()
+            return
+        line = run_reference(args, torch)
+        print(json.dumps(line), flush=True)
+        if world > 1:
+            barrier()
+            dist.destroy_process_group()
+        return
+
+    import lbm_b200 as L
+    from lbm_b200.solver import Solver
+
+    mask_np, f0_np = workload()
+    mask = torch.from_numpy(mask_np).cuda()
+    f_a = torch.from_numpy(f0_np).cuda()
+    f_b = f_a.clone()
+    S = Solver(W, H, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU)
+    T = args.T
+    n_launch = (args.frame + T - 1) // T
+    stream = torch.cuda.current_stream()
+    st = {"a": f_a, "b": f_b}
+
+    def frame():
+        for _ in range(n_launch):
+            which = S.run(st["a"], st["b"], mask, T, T)
+            if which:
+                st["a"], st["b"] = st["b"], st["a"]
+
+    for _ in range(args.warmup):
+        frame()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            frame()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    phys = args.steps * n_launch * T
+    mlups_total = W * H * phys * world / (ms * 1e3)
+    ms_per_step = ms / args.steps
+    launch_ms = ms / (args.steps * n_launch)
+
+    # End to end through the public API with host buffers: every step uploads
+    # the state and mask from pinned host memory, runs the frame and reads back
+    # u, v, rho of the last step.
+    host_f = torch.from_numpy(f0_np).pin_memory()
+    host_m = torch.from_numpy(mask_np).pin_memory()
+    host_mac = [torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in range(3)]
+    dev_mac = [torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in range(3)]
+    e2e_steps = max(3, args.steps // 3)
+
+    def e2e_step():
+        st["a"].copy_(host_f, non_blocking=True)
+        mask.copy_(host_m, non_blocking=True)
+        for li in range(n_launch):
+            last = li == n_launch - 1
+            which = S.run(st["a"], st["b"], mask, T, T, *(dev_mac if last else (None, None, None)))
+            if which:
+                st["a"], st["b"] = st["b"], st["a"]
+        for h_, d_ in zip(host_mac, dev_mac):
+            h_.copy_(d_, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(e2.elapsed_time(e3))
+    e2e_mlups = W * H * e2e_steps * n_launch * T * world / (e2e_ms * 1e3)
+    h2d = host_f.numel() * host_f.element_size() + host_m.numel()
+    d2h = sum(t.numel() * t.element_size() for t in host_mac)
+
+    flags = L.solver.device_error_flags(clear=True)
+    if rank == 0:
+        peak, peak_src = hbm_peak()
+        achieved = B_ALG * W * H * T / (launch_ms * 1e-3) / 1e9
+        traffic = None
+        tfile = os.path.join(ROOT, "profiles", "wave_kernel_T4_4096x1024_traffic.json")
+        if os.path.exists(tfile):
+            try:
+                traffic = json.load(open(tfile))["dram_bytes_per_launch"]
+            except Exception:
+                traffic = None
+        line = {
+            "metric": "MLUPS", "value": round(mlups_total, 1), "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"cylinder channel {W}x{H} D2Q9 MRT+Smagorinsky Cs={CS}, Zou-He u={U_IN}, "
+                                   f"D={CYL[2]} at ({CYL[0]},{CYL[1]}), nu={NU}, T={T} steps per launch",
+                       "W": W, "H": H, "T": T, "physical_steps_per_step": n_launch * T,
+                       "l2": "inputs larger than L2 (two 151 MB population buffers)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "e2e": {"value": round(e2e_mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "kernel": "wave_kernel (MRT+Smagorinsky, T steps per launch)",
+                         "note": f"achieved = 72 B per lattice update x W*H*T / launch time; peak {peak_src}"},
+            "gpu_launches": args.steps * n_launch,
+            "clocks": clk.summary(),
+            "device_error_flags": flags,
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline()
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        barrier()
+        dist.destroy_process_group()
+
+
+def run_reference(args, torch):
+    """fused_lbmkernel of lbm_core4.cu (compiled from source into oracle/_ref)."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_core4.so")
+    if not os.path.exists(path):
+        return {"impl": "reference", "unavailable": "oracle/_ref/libref_core4.so was not built"}
+    lib = C.CDLL(path)
+    P, I_, F = C.c_void_p, C.c_int, C.c_float
+    lib.ref_core4_step.argtypes = [P] * 6 + [I_, I_, F, F, F, P]
+    mask_np, f0_np = workload()
+    mask = torch.from_numpy(mask_np).cuda()
+    a = torch.from_numpy(f0_np).cuda()
+    b = a.clone()
+    mac = [torch.zeros((H, W), dtype=torch.float32, device="cuda") for _ in range(3)]
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    st = {"a": a, "b": b}
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+
+    def frame():
+        for _ in range(args.frame):
+            rc = lib.ref_core4_step(ptr(mask), ptr(st["a"]), ptr(st["b"]), *[ptr(t) for t in mac], W, H,
+                                    1.0 / TAU, U_IN, 1.0 / TAU, sp)
+            if rc:
+                raise RuntimeError(f"reference launch failed: {rc}")
+            st["a"], st["b"] = st["b"], st["a"]
+
+    for _ in range(args.warmup):
+        frame()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            frame()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    mlups = W * H * args.steps * args.frame / (ms * 1e3)
+    return {
+        "impl": "reference", "metric": "MLUPS", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"cylinder channel {W}x{H} D2Q9 MRT+Smagorinsky (reference constants: Cs=0.20, "
+                               f"s=1.1), Zou-He u={U_IN}, T=1 step per launch (lbm_core4.cu)",
+                   "W": W, "H": H, "physical_steps_per_step": args.frame},
+        "cpu_baseline": {"value": round(mlups, 1), "unit": "MLUPS", "cores": 0, "kind": "reference",
+                         "sample": "the reference's own CUDA kernel (oracle/_ref/libref_core4.so) on the GPU; "
+                                   "the reference has no CPU implementation of this path"},
+        "e2e": {"value": round(mlups, 1), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "gpu_launches": args.steps * args.frame,
+        "clocks": clk.summary(),
+    }
+
+
+if __name__ == "__main__":
+    main()

@@ -21,7 +21,7 @@
 // phase reads one 16-bit code instead of nine mask bytes.  Two CTAs fit per SM.
 #pragma once
 
-#include "collide.cuh"
+#include "wave.cuh" // IntC
 
 namespace lbm {
 
@@ -51,7 +51,10 @@ template <int T_, int VAR_> struct AaCfg {
     static constexpr int OFF_F = 128;
     static constexpr int OFF_M = OFF_F + 9 * PL * 4;
     static constexpr int OFF_C = OFF_M + round_up(MW * SY, 128);
-    static constexpr int SMEM = OFF_C + SX * SY * 2;
+    static constexpr int OFF_LU = OFF_C + SX * SY * 2;
+    static constexpr int OFF_DUM = OFF_LU + SY * 4;
+    static constexpr int SMEM = OFF_DUM + 9 * NT * 4;
+    static constexpr int BATCH = 4;
     static constexpr uint32_t TX = 9 * PL * 4 + MW * SY;
     static_assert(T % 2 == 0 && T >= 2 && CY > 0, "T");
     static_assert(SMEM <= 113 * 1024, "two CTAs per SM");
@@ -156,29 +159,132 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
         collide<PhysBgkRef>(f, x == 0, y, p.k, r, u, v);
     };
 
+    // Inlet velocity of each tile row (only the tile holding column 0 uses it).
+    float *lu_row = reinterpret_cast<float *>(smem + C::OFF_LU);
+    float *dummy = reinterpret_cast<float *>(smem + C::OFF_DUM) + tid; // per-thread write-only sink
+    if (tid < SY)
+        lu_row[tid] = inlet_u(p.k, yt + tid);
+    __syncthreads();
+
+    // Cells are processed in batches of C::BATCH rows per thread: all loads,
+    // then all collisions, then all stores, so the independent cells overlap.
+    // Inactive cells read from a cell inside the margin and write to the sink.
+    constexpr int NB = C::BATCH;
+
     // A phase at margin m: local collide, reversed store.
-    auto phase_a = [&](int m) {
+    auto phase_a = [&](auto zh_tag, int m) {
+        constexpr bool ZH = decltype(zh_tag)::value;
 #pragma unroll
-        for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
-            const int r = rb + 4 * j, c = col;
-            if (r < m || r >= SY - m || c < m || c >= SX - m)
-                continue;
-            if (!(code[r * SX + c] & AA_UPD))
-                continue;
-            float f[9];
+        for (int b = 0; b < C::ROWS_PER_THREAD; b += NB) {
+            float f[NB][9];
+            bool act[NB];
 #pragma unroll
-            for (int q = 0; q < 9; ++q)
-                f[q] = sl(q, c, r);
-            bgk_cell(f, xt + c, yt + r);
+            for (int jj = 0; jj < NB; ++jj) {
+                const int r = rb + 4 * (b + jj), c = col;
+                act[jj] = r >= m && r < SY - m && c >= m && c < SX - m && (code[r * SX + c] & AA_UPD);
 #pragma unroll
-            for (int q = 0; q < 9; ++q)
-                sl(opp(q), c, r) = f[q];
+                for (int q = 0; q < 9; ++q)
+                    f[jj][q] = sl(q, c, r);
+            }
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj) {
+                const int r = rb + 4 * (b + jj);
+                float rr, uu, vv;
+                collide_bf<PhysBgkRef, ZH>(f[jj], ZH && (xt + col == 0), ZH ? lu_row[r] : 0.0f, p.k, rr, uu, vv);
+            }
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj) {
+                const int r = rb + 4 * (b + jj), c = col;
+#pragma unroll
+                for (int q = 0; q < 9; ++q)
+                    *(act[jj] ? &sl(opp(q), c, r) : dummy + q * C::NT) = f[jj][q];
+            }
         }
     };
 
-    // B phase at margin m: gather, collide, scatter (into smem, or for the
-    // policy variant's last stage straight into f_out).
-    auto phase_b = [&](int m, bool to_global) {
+    // B phase at margin m >= 1 into shared memory: gather, collide, scatter.
+    // A warp whose cells are all interior fluid (or outside the margin) takes the
+    // fast body: plain gather and scatter; otherwise bounce-back and the inlet's
+    // discard slot are resolved per population.
+    auto phase_b = [&](auto zh_tag, int m) {
+        constexpr bool ZH = decltype(zh_tag)::value;
+#pragma unroll
+        for (int b = 0; b < C::ROWS_PER_THREAD; b += NB) {
+            float f[NB][9];
+            bool act[NB];
+            uint16_t cdv[NB];
+            int rr_[NB], cc_[NB];
+            bool ok = true;
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj) {
+                const int r0 = rb + 4 * (b + jj), c0 = col;
+                const bool in = r0 >= m && r0 < SY - m && c0 >= m && c0 < SX - m;
+                rr_[jj] = in ? r0 : m;
+                cc_[jj] = in ? c0 : m;
+                const uint16_t cd = code[rr_[jj] * SX + cc_[jj]];
+                act[jj] = in && (cd & AA_UPD);
+                cdv[jj] = cd;
+                ok = ok && (!in || (cd == AA_UPD && !(ZH && xt + c0 == 0)));
+            }
+            const bool fast = __all_sync(0xffffffffu, ok);
+            if (fast) {
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj)
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        f[jj][q] = sl(opp(q), cc_[jj] - cx(q), rr_[jj] - cy(q));
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj) {
+                    float r_, u_, v_;
+                    collide_bf<PhysBgkRef, false>(f[jj], false, 0.0f, p.k, r_, u_, v_);
+                }
+#pragma unroll
+                for (int jj = 0; jj < NB; ++jj) {
+                    const int r = rr_[jj], c = cc_[jj];
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        *(act[jj] ? &sl(q, c + cx(q), r + cy(q)) : dummy + q * C::NT) = f[jj][q];
+                }
+                continue;
+            }
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj) {
+                const int r = rr_[jj], c = cc_[jj];
+                const uint16_t cd = cdv[jj];
+#pragma unroll
+                for (int q = 0; q < 9; ++q)
+                    f[jj][q] = (cd & (1u << q)) ? sl(q, c, r) : sl(opp(q), c - cx(q), r - cy(q));
+            }
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj) {
+                const int r = rb + 4 * (b + jj);
+                float r_, u_, v_;
+                collide_bf<PhysBgkRef, ZH>(f[jj], ZH && (xt + col == 0), ZH ? lu_row[r] : 0.0f, p.k, r_, u_, v_);
+            }
+#pragma unroll
+            for (int jj = 0; jj < NB; ++jj) {
+                const int r = rr_[jj], c = cc_[jj];
+                const uint16_t cd = cdv[jj];
+                const bool left = xt + c == 0;
+#pragma unroll
+                for (int q = 0; q < 9; ++q) {
+                    float *dst;
+                    if (cx(q) < 0 && left)
+                        dst = &sl(q, c + cx(q), r + cy(q)); // discard slot left of the inlet
+                    else if (q && (cd & (1u << opp(q))))   // x + c_q is solid: bounce back
+                        dst = &sl(opp(q), c, r);
+                    else
+                        dst = &sl(q, c + cx(q), r + cy(q));
+                    *(act[jj] ? dst : dummy + q * C::NT) = f[jj][q];
+                }
+            }
+        }
+    };
+
+    // Policy B-final at margin T-1: gather, collide, scatter straight into f_out
+    // (lbm_core_smemaa_policy.cu:338-424).
+    auto phase_b_final = [&](int m) {
+        const long long N = (long long)W * H;
 #pragma unroll
         for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
             const int r = rb + 4 * j, c = col;
@@ -193,66 +299,60 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
             for (int q = 0; q < 9; ++q)
                 f[q] = (cd & (1u << q)) ? sl(q, c, r) : sl(opp(q), c - cx(q), r - cy(q));
             bgk_cell(f, x, y);
-            if (!to_global) {
 #pragma unroll
-                for (int q = 0; q < 9; ++q) {
-                    if (x == 0 && cx(q) < 0)
-                        sl(q, c + cx(q), r + cy(q)) = f[q]; // discard slot left of the inlet
-                    else if (q && (cd & (1u << opp(q))))  // x + c_q is solid: bounce back
-                        sl(opp(q), c, r) = f[q];
-                    else
-                        sl(q, c + cx(q), r + cy(q)) = f[q];
+            for (int q = 0; q < 9; ++q) {
+                if (x == 0 && cx(q) < 0)
+                    continue;
+                int tx, ty, tq;
+                if (q && (cd & (1u << opp(q)))) {
+                    tx = x;
+                    ty = y;
+                    tq = opp(q);
+                } else {
+                    tx = x + cx(q);
+                    ty = y + cy(q);
+                    tq = q;
                 }
-            } else {
-                // B-final scatter, lbm_core_smemaa_policy.cu:387-421.
-                const long long N = (long long)W * H;
-#pragma unroll
-                for (int q = 0; q < 9; ++q) {
-                    if (x == 0 && cx(q) < 0)
-                        continue;
-                    int tx, ty, tq;
-                    if (q && (cd & (1u << opp(q)))) {
-                        tx = x;
-                        ty = y;
-                        tq = opp(q);
-                    } else {
-                        tx = x + cx(q);
-                        ty = y + cy(q);
-                        tq = q;
-                    }
-                    if (tx == W - 1)
-                        continue;
-                    if (tx < xt + T || tx >= xt + T + CX || ty < yt + T || ty >= yt + T + CY || tx < 0 || tx >= W ||
-                        ty < 0 || ty >= H)
-                        continue;
-                    float *dst = p.f_out + tq * N + (long long)ty * W + tx;
-                    dst[0] = f[q];
-                    if (tx == W - 2)
-                        dst[1] = f[q];
-                }
+                if (tx == W - 1)
+                    continue;
+                if (tx < xt + T || tx >= xt + T + CX || ty < yt + T || ty >= yt + T + CY || tx < 0 || tx >= W ||
+                    ty < 0 || ty >= H)
+                    continue;
+                float *dst = p.f_out + tq * N + (long long)ty * W + tx;
+                dst[0] = f[q];
+                if (tx == W - 2)
+                    dst[1] = f[q];
             }
         }
     };
 
-    for (int pr = 0; pr < T / 2; ++pr) {
-        phase_a(2 * pr);
-        __syncthreads();
-        if (has_outlet) {
-            ghost_copy();
+    auto run = [&](auto zh_tag) {
+        for (int pr = 0; pr < T / 2; ++pr) {
+            phase_a(zh_tag, 2 * pr);
             __syncthreads();
-        }
-        const bool last = pr == T / 2 - 1;
-        if (C::VAR == VARIANT_POLICY && last) {
-            phase_b(2 * pr + 1, true);
-            return;
-        }
-        phase_b(2 * pr + 1, false);
-        __syncthreads();
-        if (C::VAR == VARIANT_SMEMAA && has_outlet) {
-            ghost_copy();
+            if (has_outlet) {
+                ghost_copy();
+                __syncthreads();
+            }
+            const bool last = pr == T / 2 - 1;
+            if (C::VAR == VARIANT_POLICY && last) {
+                phase_b_final(2 * pr + 1);
+                return;
+            }
+            phase_b(zh_tag, 2 * pr + 1);
             __syncthreads();
+            if (C::VAR == VARIANT_SMEMAA && has_outlet) {
+                ghost_copy();
+                __syncthreads();
+            }
         }
-    }
+    };
+    if (xt <= 0)
+        run(IntC<1>{});
+    else
+        run(IntC<0>{});
+    if (C::VAR == VARIANT_POLICY)
+        return;
 
     // ---- smemaa epilogue: canonical core and u, v, rho (lbm_core_smemaa.cu:500-546) ----
     const long long N = (long long)W * H;
@@ -272,9 +372,10 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
             p.f_out[q * N + id] = f[q];
         }
         if (!solid(c, r) && x < W - 1 && y > 0 && y < H - 1) {
-            const float rr = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
-            p.ux[id] = ((f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7])) / rr;
-            p.uy[id] = ((f[2] - f[4]) + (f[5] + f[6]) - (f[7] + f[8])) / rr;
+            float rr, uu, vv;
+            moments_seq(f, rr, uu, vv);
+            p.ux[id] = uu;
+            p.uy[id] = vv;
             p.rho[id] = rr;
         }
     }

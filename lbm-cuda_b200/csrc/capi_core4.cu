@@ -2,7 +2,7 @@
 // per-cell auxiliary kernels (macro extraction, vorticity colour map).
 #include <string.h>
 
-#include "wave_launch.cuh"
+#include "dispatch.cuh"
 
 namespace lbm {
 
@@ -60,30 +60,9 @@ static WaveParams core4_params(const uint8_t *mask, const float *f_now, float *f
     return p;
 }
 
-template <int T, int NX> using Core4Cfg = WaveCfg<T, NX, PhysCore4, StoreF32, MODE_CORE4>;
-
 static int core4_launch(const WaveParams &p, int T, cudaStream_t s)
 {
-    switch (T) {
-    case 1:
-        return launch_wave<Core4Cfg<1, 224>>(p, s);
-    case 2:
-        return launch_wave<Core4Cfg<2, 128>>(p, s);
-    case 3:
-        return launch_wave<Core4Cfg<3, 128>>(p, s);
-    case 4:
-        return launch_wave<Core4Cfg<4, 128>>(p, s);
-    case 5:
-        return launch_wave<Core4Cfg<5, 128>>(p, s);
-    case 6:
-        return launch_wave<Core4Cfg<6, 128>>(p, s);
-    case 7:
-        return launch_wave<Core4Cfg<7, 128>>(p, s);
-    case 8:
-        return launch_wave<Core4Cfg<8, 128>>(p, s);
-    default:
-        return LBM_ERR_UNSUPPORTED;
-    }
+    return launch_step<PhysCore4, StoreF32, MODE_CORE4>(p, T, s);
 }
 
 // macro_kernel semantics (lbm_core_smemaa_policy.cu:431-476).
@@ -102,9 +81,8 @@ __global__ void macro_kernel(const float *__restrict__ f, float *__restrict__ ux
 #pragma unroll
     for (int q = 0; q < 9; ++q)
         fl[q] = f[q * N + pid];
-    float r = ((fl[0] + fl[1]) + (fl[2] + fl[3])) + ((fl[4] + fl[5]) + (fl[6] + fl[7])) + fl[8];
-    float u = ((fl[1] - fl[3]) + (fl[5] - fl[6]) + (fl[8] - fl[7])) / r;
-    float v = ((fl[2] - fl[4]) + (fl[5] + fl[6]) - (fl[7] + fl[8])) / r;
+    float r, u, v;
+    moments_seq(fl, r, u, v);
     if (x == 0) {
         const float lu = inlet_u(k, y);
         r = zou_he(fl, lu);

@@ -4,11 +4,12 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include "wave_launch.cuh"
+#include "dispatch.cuh"
 
 struct lbm_handle {
     lbm_params p;
     lbm::Phys k;
+    int variant;      // VAR_* compile-time physics variant
     double *partials; // reduction scratch: kRedBlocks x 3 doubles
 };
 
@@ -16,32 +17,6 @@ namespace lbm {
 
 constexpr int kRedBlocks = 296; // fixed, so that the FP64 reductions are deterministic
 constexpr int kRedThreads = 256;
-
-template <class St, int T, int NX> using GenCfg = WaveCfg<T, NX, PhysRuntime, St, MODE_GENERAL>;
-
-template <class St> static int general_launch(const WaveParams &p, int T, cudaStream_t s)
-{
-    switch (T) {
-    case 1:
-        return launch_wave<GenCfg<St, 1, 224>>(p, s);
-    case 2:
-        return launch_wave<GenCfg<St, 2, 128>>(p, s);
-    case 3:
-        return launch_wave<GenCfg<St, 3, 128>>(p, s);
-    case 4:
-        return launch_wave<GenCfg<St, 4, 128>>(p, s);
-    case 5:
-        return launch_wave<GenCfg<St, 5, 128>>(p, s);
-    case 6:
-        return launch_wave<GenCfg<St, 6, 128>>(p, s);
-    case 7:
-        return launch_wave<GenCfg<St, 7, 128>>(p, s);
-    case 8:
-        return launch_wave<GenCfg<St, 8, 128>>(p, s);
-    default:
-        return LBM_ERR_UNSUPPORTED;
-    }
-}
 
 static int elem_bytes(int storage)
 {
@@ -182,6 +157,21 @@ template <class F> static int by_storage(int storage, F &&fn)
     }
 }
 
+// Compile-time physics variant of a parameter set, or -1 if none is built.
+static int variant_of(const lbm_params &p)
+{
+    int v = -1;
+    if (p.collision == LBM_COLL_MRT && p.closure == LBM_CLOSURE_SMAG)
+        v = (p.u_lid != 0.0f) ? -1 : (p.ref_clamps ? VAR_MRT_SMAG_CLAMP : VAR_MRT_SMAG);
+    else if (p.collision == LBM_COLL_MRT && p.closure == LBM_CLOSURE_NONE && !p.ref_clamps)
+        v = (p.u_lid != 0.0f) ? VAR_MRT_LID : VAR_MRT;
+    else if (p.collision == LBM_COLL_BGK && p.closure == LBM_CLOSURE_NONE && !p.ref_clamps && p.u_lid == 0.0f)
+        v = VAR_BGK;
+    if (p.storage != LBM_STORE_F32 && (v == VAR_MRT_LID || v == VAR_BGK))
+        v = -1;
+    return v;
+}
+
 static int validate(const lbm_params *p)
 {
     if (!p || p->W < 3 || p->H < 3)
@@ -205,6 +195,8 @@ static int validate(const lbm_params *p)
         return LBM_ERR_ARG;
     if (y != LBM_BC_WALL && y != LBM_BC_PERIODIC)
         return LBM_ERR_ARG;
+    if (variant_of(*p) < 0)
+        return LBM_ERR_UNSUPPORTED;
     return LBM_OK;
 }
 
@@ -274,6 +266,7 @@ int lbm_create(const lbm_params *p, lbm_handle **out)
         return LBM_ERR_ARG;
     h->p = *p;
     h->k = make_phys(*p);
+    h->variant = variant_of(*p);
     cudaError_t e = cudaMalloc(&h->partials, sizeof(double) * 3 * kRedBlocks);
     if (e != cudaSuccess) {
         free(h);
@@ -344,7 +337,13 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
         wp.bc_y = h->p.bc_y;
         wp.use_tma = 1;
         wp.k = h->k;
-        int rc = by_storage(h->p.storage, [&](auto st) { return general_launch<decltype(st)>(wp, t, s); });
+        int rc = LBM_ERR_ARG;
+        if (h->p.storage == LBM_STORE_F32)
+            rc = general_launch_f32(h->variant, wp, t, s);
+        else if (h->p.storage == LBM_STORE_F16DEV)
+            rc = general_launch_f16(h->variant, wp, t, s);
+        else if (h->p.storage == LBM_STORE_BF16DEV)
+            rc = general_launch_bf16(h->variant, wp, t, s);
         if (rc)
             return rc;
         done += t;

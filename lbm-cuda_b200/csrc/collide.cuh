@@ -51,7 +51,12 @@ template <bool kMrt_, bool kSmag_, bool kClampU_, bool kClampF_, bool kInletSmag
 using PhysCore4 = Physics<true, true, true, true, false>;
 // lbm_core_smemaa*.cu semantics: BGK, population clamp only.
 using PhysBgkRef = Physics<false, false, false, true, false>;
-// General solver: the same choices read from Phys::flags (uniform branches).
+// General solver variants.
+using PhysMrtSmagClamp = Physics<true, true, true, true, false>; // = PhysCore4 with runtime rates and Cs
+using PhysMrtSmag = Physics<true, true, false, false, false>;
+using PhysMrt = Physics<true, false, false, false, false>;
+using PhysBgk = Physics<false, false, false, false, false>;
+// The same choices read from Phys::flags (uniform branches; non-hot paths).
 struct PhysRuntime {
     static constexpr bool kRuntime = true;
     static constexpr bool kMrt = true, kSmag = true, kClampU = true, kClampF = true, kInletSmag = true;
@@ -138,6 +143,17 @@ __device__ __forceinline__ void bgk_relax(float (&f)[9], float r, float u, float
     }
 }
 
+// rho, u, v with the reference's summation order (sequential over q,
+// lbm_core4.cu:130-141), so that FP32 rounding follows the reference.
+__device__ __forceinline__ void moments_seq(const float (&f)[9], float &r, float &u, float &v)
+{
+    r = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
+    const float jx = f[1] - f[3] + f[5] - f[6] - f[7] + f[8];
+    const float jy = f[2] - f[4] + f[5] + f[6] - f[7] - f[8];
+    u = jx / r;
+    v = jy / r;
+}
+
 // Full collision of one updated cell.  `inlet` selects the Zou-He branch
 // (x = 0, prescribed velocity); r/u/v receive the macroscopic values the
 // reference writes to its rho/ux/uy arrays.
@@ -149,11 +165,7 @@ __device__ __forceinline__ void collide(float (&f)[9], bool inlet, int y, const 
     const bool kClampU = Ph::kRuntime ? (k.flags & PF_CLAMPU) != 0 : Ph::kClampU;
     const bool kClampF = Ph::kRuntime ? (k.flags & PF_CLAMPF) != 0 : Ph::kClampF;
     const bool kInletSmag = Ph::kRuntime ? (k.flags & PF_INLET_SMAG) != 0 : Ph::kInletSmag;
-    r = ((f[0] + f[1]) + (f[2] + f[3])) + ((f[4] + f[5]) + (f[6] + f[7])) + f[8];
-    const float jx = (f[1] - f[3]) + (f[5] - f[6]) + (f[8] - f[7]);
-    const float jy = (f[2] - f[4]) + (f[5] + f[6]) - (f[7] + f[8]);
-    u = jx / r;
-    v = jy / r;
+    moments_seq(f, r, u, v);
     if (kClampU) {
         u = fminf(0.4f, fmaxf(-0.4f, u));
         v = fminf(0.4f, fmaxf(-0.4f, v));
@@ -175,6 +187,52 @@ __device__ __forceinline__ void collide(float (&f)[9], bool inlet, int y, const 
     else
         bgk_relax(f, r, u, v, s);
     if (kClampF) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+            f[q] = fminf(10.0f, fmaxf(0.0f, f[q]));
+    }
+}
+
+// Branch-free collision for the wavefront kernel's hot loop: the Zou-He values
+// are computed for every cell and selected where `inlet` holds (kZh = false
+// drops them at compile time for strips without the inlet column), so that the
+// scheduler can interleave the independent cells of several time levels.
+// `lu` is the inlet velocity of the cell's row.
+template <class Ph, bool kZh>
+__device__ __forceinline__ void collide_bf(float (&f)[9], bool inlet, float lu, const Phys &k, float &r, float &u,
+                                           float &v)
+{
+    static_assert(!Ph::kRuntime, "compile-time physics only");
+    moments_seq(f, r, u, v);
+    if (Ph::kClampU) {
+        u = fminf(0.4f, fmaxf(-0.4f, u));
+        v = fminf(0.4f, fmaxf(-0.4f, v));
+        r = fminf(1.5f, fmaxf(0.0f, r));
+    }
+    if (kZh) {
+        const float rz = (f[0] + f[2] + f[4] + 2.0f * (f[3] + f[6] + f[7])) / (1.0f - lu);
+        const float a = 0.16666666666f * rz * lu;
+        const float h = 0.5f * (f[2] - f[4]);
+        const float z1 = f[3] + 0.666666667f * rz * lu;
+        const float z5 = f[7] - h + a;
+        const float z8 = f[6] + h + a;
+        f[1] = inlet ? z1 : f[1];
+        f[5] = inlet ? z5 : f[5];
+        f[8] = inlet ? z8 : f[8];
+        r = inlet ? rz : r;
+        u = inlet ? lu : u;
+        v = inlet ? 0.0f : v;
+    }
+    float s = k.s_nu;
+    if (Ph::kSmag) {
+        const float sm = smag_rate(f, r, u, v, k);
+        s = (kZh && inlet && !Ph::kInletSmag) ? k.s_nu : sm;
+    }
+    if (Ph::kMrt)
+        mrt_relax(f, r, u, v, k.s_e, k.s_eps, k.s_q, s);
+    else
+        bgk_relax(f, r, u, v, s);
+    if (Ph::kClampF) {
 #pragma unroll
         for (int q = 0; q < 9; ++q)
             f[q] = fminf(10.0f, fmaxf(0.0f, f[q]));

@@ -1,0 +1,65 @@
+// Kernel selection for one launch of T fused steps: the 128-bit streaming
+// kernel for aligned single steps, the wavefront kernel otherwise.
+#pragma once
+
+#include "stream.cuh"
+#include "wave_launch.cuh"
+
+namespace lbm {
+
+// General-solver physics variants (lbm_params -> compile-time choices).
+enum : int { VAR_MRT_SMAG_CLAMP = 0, VAR_MRT_SMAG = 1, VAR_MRT = 2, VAR_MRT_LID = 3, VAR_BGK = 4 };
+
+template <class C> int launch_stream(WaveParams p, cudaStream_t s)
+{
+    if (!p.err)
+        p.err = device_error_word();
+    dim3 grid((p.W + 127) / 128, (p.H + 3) / 4);
+    dim3 block(32, 4);
+    stream_kernel<C><<<grid, block, 0, s>>>(p);
+    return status(cudaGetLastError());
+}
+
+inline bool stream_ok(const WaveParams &p)
+{
+    auto a4 = [](const void *q) { return (reinterpret_cast<uintptr_t>(q) & 3u) == 0; };
+    bool ok = p.W % 4 == 0 && p.pitch % 4 == 0 && p.plane % 4 == 0 && aligned16(p.f_in) && aligned16(p.f_out) &&
+              a4(p.mask) && p.mask_pitch % 4 == 0;
+    if (p.ux)
+        ok = ok && aligned16(p.ux) && aligned16(p.uy) && aligned16(p.rho);
+    return ok;
+}
+
+template <class Ph, class St, int MODE, bool LID = false>
+int launch_step(const WaveParams &p, int T, cudaStream_t s)
+{
+    if (T == 1 && stream_ok(p))
+        return launch_stream<StreamCfg<Ph, St, MODE, LID>>(p, s);
+    switch (T) {
+    case 1:
+        return launch_wave<WaveCfg<1, 224, Ph, St, MODE, LID>>(p, s);
+    case 2:
+        return launch_wave<WaveCfg<2, 128, Ph, St, MODE, LID>>(p, s);
+    case 3:
+        return launch_wave<WaveCfg<3, 128, Ph, St, MODE, LID>>(p, s);
+    case 4:
+        return launch_wave<WaveCfg<4, 128, Ph, St, MODE, LID>>(p, s);
+    case 5:
+        return launch_wave<WaveCfg<5, 128, Ph, St, MODE, LID>>(p, s);
+    case 6:
+        return launch_wave<WaveCfg<6, 128, Ph, St, MODE, LID>>(p, s);
+    case 7:
+        return launch_wave<WaveCfg<7, 128, Ph, St, MODE, LID>>(p, s);
+    case 8:
+        return launch_wave<WaveCfg<8, 128, Ph, St, MODE, LID>>(p, s);
+    default:
+        return LBM_ERR_UNSUPPORTED;
+    }
+}
+
+// Defined in general_*.cu (one translation unit per storage format).
+int general_launch_f32(int variant, const WaveParams &p, int T, cudaStream_t s);
+int general_launch_f16(int variant, const WaveParams &p, int T, cudaStream_t s);
+int general_launch_bf16(int variant, const WaveParams &p, int T, cudaStream_t s);
+
+} // namespace lbm

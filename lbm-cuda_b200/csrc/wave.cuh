@@ -62,8 +62,9 @@ struct WaveParams {
     Phys k;
 };
 
-template <int T_, int NX_, class Ph_, class St_, int MODE_> struct WaveCfg {
+template <int T_, int NX_, class Ph_, class St_, int MODE_, bool LID_ = false> struct WaveCfg {
     static constexpr int T = T_;
+    static constexpr bool LID = LID_;
     static constexpr int NX = NX_;
     static constexpr int CW = NX - 2 * T;
     static constexpr int MODE = MODE_;
@@ -75,9 +76,10 @@ template <int T_, int NX_, class Ph_, class St_, int MODE_> struct WaveCfg {
     static constexpr int RW = NX + 2 * AE;          // input row width (covers xs-1 .. xs+NX)
     static constexpr int RWM = NX + 32;             // mask row width (bytes)
     static constexpr int LW = NX + 2;               // level ring row width
-    static constexpr int P = (T == 1) ? 4 : 3;      // TMA prefetch distance (rows)
-    static constexpr int DI = P + 4;                // input ring depth
-    static constexpr int DC = 2 * T;                // code ring depth
+    static constexpr int P = 4;                     // TMA prefetch distance (rows)
+    static constexpr int DI = P + 4;                // input ring depth (power of two)
+    static constexpr int DC = (2 * T <= 2) ? 2 : ((2 * T <= 4) ? 4 : ((2 * T <= 8) ? 8 : 16)); // code ring depth
+    static_assert((DI & (DI - 1)) == 0 && DC >= 2 * T, "ring depths");
     static constexpr int NLV = (T > 1) ? (T - 1) : 0;
     static constexpr int SLOT_F = round_up(9 * RW * ES, 128); // bytes per input row
     static constexpr int SLOT_M = round_up(RWM, 128);
@@ -86,7 +88,9 @@ template <int T_, int NX_, class Ph_, class St_, int MODE_> struct WaveCfg {
     static constexpr int OFF_M = OFF_IN + DI * SLOT_F;
     static constexpr int OFF_L = OFF_M + DI * SLOT_M;
     static constexpr int OFF_C = OFF_L + NLV * 4 * 9 * LW * 4;
-    static constexpr int SMEM = OFF_C + DC * NX * 4;
+    static constexpr int OFF_LU = OFF_C + DC * NX * 4;
+    static constexpr int OFF_DUM = OFF_LU + round_up(DC * 4, 16); // write-only sink, 2 x 9 x NX floats
+    static constexpr int SMEM = OFF_DUM + 2 * 9 * NX * 4;
     static constexpr uint32_t TX_BYTES = 9 * RW * ES + RWM;
     static constexpr int MINB = (SMEM <= 74 * 1024) ? 3 : ((SMEM <= 112 * 1024) ? 2 : 1);
     static_assert(NX % 32 == 0 && CW > 0, "strip");
@@ -94,6 +98,19 @@ template <int T_, int NX_, class Ph_, class St_, int MODE_> struct WaveCfg {
     static_assert(SMEM <= 227 * 1024, "shared memory");
     static_assert(DI * 8 <= 120, "mbarriers and the abort flag share the first 128 bytes");
 };
+
+template <int V> struct IntC {
+    static constexpr int value = V;
+};
+
+// Compile-time loop: f(IntC<I>{}) for I in [I0, I1).
+template <int I0, int I1, class F> __device__ __forceinline__ void static_for(F &&f)
+{
+    if constexpr (I0 < I1) {
+        f(IntC<I0>{});
+        static_for<I0 + 1, I1>(f);
+    }
+}
 
 // Mask value of the 3x3 neighbourhood entry (dx, dy) in {-1,0,1}^2.
 struct Nbhd {
@@ -185,6 +202,7 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
     unsigned char *m_base = smem + C::OFF_M;
     float *lvl = reinterpret_cast<float *>(smem + C::OFF_L);
     uint32_t *code = reinterpret_cast<uint32_t *>(smem + C::OFF_C);
+    float *lu_ring = reinterpret_cast<float *>(smem + C::OFF_LU);
     volatile int &s_abort = *reinterpret_cast<int *>(smem + C::OFF_BAR + 124);
 
     const int i = threadIdx.x;
@@ -204,9 +222,10 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
     const int xm0 = tma ? floor_div(xs - 1, 16) * 16 : xs - 1;
     const int of = xs - xf0;
     const int om = xs - xm0;
+    const bool colcore = i >= T && i < T + CW && x < p.W;
 
-    auto in_row = [&](int r) -> E * { return reinterpret_cast<E *>(in_base + ((r - row0) % DI) * C::SLOT_F); };
-    auto m_row = [&](int r) -> uint8_t * { return m_base + ((r - row0) % DI) * C::SLOT_M; };
+    auto in_row = [&](int r) -> E * { return reinterpret_cast<E *>(in_base + ((r - row0) & (DI - 1)) * C::SLOT_F); };
+    auto m_row = [&](int r) -> uint8_t * { return m_base + ((r - row0) & (DI - 1)) * C::SLOT_M; };
     auto lv_row = [&](int t, int r) -> float * { return lvl + ((t - 1) * 4 + ((r - row0) & 3)) * 9 * LW; };
 
     if (i == 0) {
@@ -224,7 +243,7 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
     __syncthreads();
 
     auto issue_row = [&](int r) { // thread 0, TMA path
-        const int s = (r - row0) % DI;
+        const int s = (r - row0) & (DI - 1);
         const int ry = pyper ? wrap(r, p.H) : r;
         mbar_arrive_expect_tx(&mbar[s], C::TX_BYTES);
         tma_load_3d(in_base + s * C::SLOT_F, &tmf, &mbar[s], xf0, ry, 0);
@@ -250,7 +269,7 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
         }
     };
 
-    int next_wait = row0; // thread-local: next input row this thread waits for (TMA path)
+    int next_wait = row0;  // next input row this thread waits for (TMA path)
     int issued_end = row0; // thread 0: one past the last issued row
     if (tma) {
         if (i == 0) {
@@ -279,118 +298,174 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
             c = build_code_core4(n, x, r, p.W, p.H);
         else
             c = build_code_general(n, x, r, p);
-        code[((r - row0) % DC) * NX + i] = c;
+        const int slot = (r - row0) & (DC - 1);
+        code[slot * NX + i] = c;
+        if (i == 0)
+            lu_ring[slot] = inlet_u(p.k, pyper ? wrap(r, p.H) : r);
     };
 
-    for (int k = 0; k < K; ++k) {
-        const int r1 = ya - T + 1 + k;
-        const bool l1 = r1 <= yb + T - 2;
-        if (tma) {
-            if (l1) {
-                // Wait for every row up to r1 + 1 (rows arrive in order).
-                while (next_wait <= r1 + 1) {
-                    const int rr = next_wait - row0;
-                    if (!mbar_wait_bounded(&mbar[rr % DI], (uint32_t)((rr / DI) & 1))) {
-                        s_abort = 1;
-                        if (p.err)
-                            atomicOr(p.err, 1);
-                        break;
-                    }
-                    ++next_wait;
-                }
-                build_code(r1);
-            }
-            __syncthreads();
-            if (s_abort)
-                break;
-            if (i == 0 && l1 && r1 + 2 + P < row0 + nin) {
-                fence_proxy_async();
-                issue_row(r1 + 2 + P);
-                issued_end = r1 + 3 + P;
-            }
-        } else {
-            if (l1)
-                plain_row(r1 + 1);
-            __syncthreads();
-            if (l1)
-                build_code(r1);
-            __syncthreads();
-        }
+    // Value of level t-1 at (row rt + dr, column x + dc), population q.
+    auto src = [&](auto t_tag, int rt, int dr, int q, int dc) -> float {
+        constexpr int t = decltype(t_tag)::value;
+        if (t == 1)
+            return St::load(in_row(rt + dr)[q * RW + i + of + dc], q);
+        return lv_row(t - 1, rt + dr)[q * LW + i + 1 + dc];
+    };
 
+    // ---- level computations ----
+    // Level t at iteration k works on row r1 - 2(t-1).  All T levels are
+    // computed in every iteration (levels outside their row range compute on
+    // stale ring rows and do not store), so one straight-line body serves every
+    // iteration and the T independent cells overlap in the scheduler.
+    // Per iteration a warp vote picks the fast body (every lane's cell is
+    // interior fluid at every level: code == 0) or the generic body (bounce-back
+    // and moving walls, Zou-He inlet, pass-through of cells that are not
+    // updated, outlet ghost).  Suppressed shared-memory writes go to a dummy row.
+    float *dummy = reinterpret_cast<float *>(smem + C::OFF_DUM);
+
+    auto main_loop = [&]() {
+        for (int k = 0; k < K; ++k) {
+            const int r1 = ya - T + 1 + k;
+            const bool l1 = r1 <= yb + T - 2;
+            if (tma) {
+                if (l1) {
+                    // Wait for every row up to r1 + 1 (rows arrive in order).
+                    while (next_wait <= r1 + 1) {
+                        const int rr = next_wait - row0;
+                        if (!mbar_wait_bounded(&mbar[rr & (DI - 1)], (uint32_t)((rr / DI) & 1))) {
+                            s_abort = 1;
+                            if (p.err)
+                                atomicOr(p.err, 1);
+                            break;
+                        }
+                        ++next_wait;
+                    }
+                    build_code(r1);
+                }
+                __syncthreads();
+                if (s_abort)
+                    break;
+                if (i == 0 && l1 && r1 + 2 + P < row0 + nin) {
+                    fence_proxy_async();
+                    issue_row(r1 + 2 + P);
+                    issued_end = r1 + 3 + P;
+                }
+            } else {
+                if (l1)
+                    plain_row(r1 + 1);
+                __syncthreads();
+                if (l1)
+                    build_code(r1);
+                __syncthreads();
+            }
+
+            int rt[T];
+            bool act[T];
+            uint32_t cd[T];
+            bool special = false;
 #pragma unroll
-        for (int t = 1; t <= T; ++t) {
-            const int rt = r1 - 2 * (t - 1);
-            if (rt < ya - T + t || rt >= yb + T - t)
-                continue;
-            const uint32_t c = code[((rt - row0) % DC) * NX + i];
-            // Value of level t-1 at (row rt + dr, column x + dc), population q.
-            auto src = [&](int dr, int q, int dc) -> float {
-                if (t == 1)
-                    return St::load(in_row(rt + dr)[q * RW + i + of + dc], q);
-                return lv_row(t - 1, rt + dr)[q * LW + i + 1 + dc];
-            };
-            float *dst = (t < T) ? lv_row(t, rt) : nullptr;
-            if (c & C_SKIP) {
-                if (t < T && !(c & C_GHOST_SKIP)) {
+            for (int t = 1; t <= T; ++t) {
+                rt[t - 1] = r1 - 2 * (t - 1);
+                act[t - 1] = rt[t - 1] >= ya - T + t && rt[t - 1] < yb + T - t;
+                cd[t - 1] = code[((rt[t - 1] - row0) & (DC - 1)) * NX + i];
+                special |= act[t - 1] && cd[t - 1] != 0;
+            }
+            const bool fast = !__any_sync(0xffffffffu, special);
+
+            float f[T][9];
+            float mr[T], mu[T], mv[T];
+            if (fast) {
+                static_for<1, T + 1>([&](auto tt) {
+                    constexpr int t = decltype(tt)::value;
 #pragma unroll
                     for (int q = 0; q < 9; ++q)
-                        dst[q * LW + i + 1] = src(0, q, 0);
+                        f[t - 1][q] = src(tt, rt[t - 1], -cy(q), q, -cx(q));
+                });
+#pragma unroll
+                for (int t = 0; t < T; ++t)
+                    collide_bf<Ph, false>(f[t], false, 0.0f, p.k, mr[t], mu[t], mv[t]);
+            } else {
+                float own[T][9];
+                static_for<1, T + 1>([&](auto tt) {
+                    constexpr int t = decltype(tt)::value;
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        own[t - 1][q] = src(tt, rt[t - 1], 0, q, 0);
+                    f[t - 1][0] = own[t - 1][0];
+#pragma unroll
+                    for (int q = 1; q < 9; ++q)
+                        f[t - 1][q] = src(tt, rt[t - 1], -cy(q), q, -cx(q));
+                });
+#pragma unroll
+                for (int t = 0; t < T; ++t) {
+                    const uint32_t c = cd[t];
+#pragma unroll
+                    for (int q = 1; q < 9; ++q) {
+                        float bv = own[t][opp(q)];
+                        if (C::LID)
+                            bv += ((c >> (C_MOVING_SHIFT + q)) & 1u) ? 6.0f * wgt(q) * (float)cx(q) * p.k.u_lid : 0.0f;
+                        f[t][q] = ((c >> q) & 1u) ? bv : f[t][q];
+                    }
+                    const int slot = (rt[t] - row0) & (DC - 1);
+                    collide_bf<Ph, true>(f[t], (c & C_INLET) != 0, lu_ring[slot], p.k, mr[t], mu[t], mv[t]);
+                    const bool skip = (c & C_SKIP) != 0;
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        f[t][q] = skip ? own[t][q] : f[t][q];
                 }
-                continue;
             }
-            float f[9];
+
+            // stores: levels 1..T-1 into their rings, level T to HBM
 #pragma unroll
-            for (int q = 0; q < 9; ++q)
-                f[q] = src(-cy(q), q, -cx(q));
-            if (c & C_BOUNCE) {
+            for (int t = 1; t < T; ++t) {
+                const uint32_t c = cd[t - 1];
+                float *dst = lv_row(t, rt[t - 1]);
+                const bool wr = act[t - 1] && !(c & C_GHOST_SKIP);
+                const bool gh = act[t - 1] && (c & C_GHOST_SRC);
+                float *d1 = wr ? dst + i + 1 : dummy + i;
+                float *d2 = gh ? dst + i + 2 : dummy + 9 * NX + i;
+                const int s1 = wr ? LW : NX;
+                const int s2 = gh ? LW : NX;
 #pragma unroll
-                for (int q = 1; q < 9; ++q) {
-                    if (c & (1u << q)) {
-                        float b = src(0, opp(q), 0);
-                        if (C::MODE == MODE_GENERAL && (c & (1u << (C_MOVING_SHIFT + q))))
-                            b += 6.0f * wgt(q) * (float)cx(q) * p.k.u_lid; // Ladd, rho_w = 1
-                        f[q] = b;
+                for (int q = 0; q < 9; ++q)
+                    d1[q * s1] = f[t - 1][q];
+                if (!fast) {
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        d2[q * s2] = f[t - 1][q];
+                }
+            }
+            {
+                const uint32_t c = cd[T - 1];
+                const int r = rt[T - 1];
+                if (act[T - 1] && !(c & C_SKIP) && colcore && r >= ya && r < yb) {
+                    E *fo = reinterpret_cast<E *>(p.f_out) + (long long)r * p.pitch + x;
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        fo[q * p.plane] = St::store(f[T - 1][q], q);
+                    if (c & C_GHOST_SRC) {
+#pragma unroll
+                        for (int q = 0; q < 9; ++q)
+                            fo[q * p.plane + 1] = St::store(f[T - 1][q], q);
+                    }
+                    if (p.ux) {
+                        const long long id = (long long)r * p.W + x;
+                        p.ux[id] = mu[T - 1];
+                        p.uy[id] = mv[T - 1];
+                        p.rho[id] = mr[T - 1];
                     }
                 }
             }
-            float r, u, v;
-            const int yr = pyper ? wrap(rt, p.H) : rt;
-            collide<Ph>(f, (c & C_INLET) != 0, yr, p.k, r, u, v);
-            if (t < T) {
-#pragma unroll
-                for (int q = 0; q < 9; ++q)
-                    dst[q * LW + i + 1] = f[q];
-                if (c & C_GHOST_SRC) {
-#pragma unroll
-                    for (int q = 0; q < 9; ++q)
-                        dst[q * LW + i + 2] = f[q];
-                }
-            } else if (i >= T && i < T + CW && x < p.W && rt >= ya && rt < yb) {
-                E *fo = reinterpret_cast<E *>(p.f_out) + (long long)rt * p.pitch + x;
-#pragma unroll
-                for (int q = 0; q < 9; ++q)
-                    fo[q * p.plane] = St::store(f[q], q);
-                if (c & C_GHOST_SRC) {
-#pragma unroll
-                    for (int q = 0; q < 9; ++q)
-                        fo[q * p.plane + 1] = St::store(f[q], q);
-                }
-                if (p.ux) {
-                    const long long id = (long long)rt * p.W + x;
-                    p.ux[id] = u;
-                    p.uy[id] = v;
-                    p.rho[id] = r;
-                }
-            }
         }
-    }
+    };
+    main_loop();
 
     // Abort path: wait (bounded) for copies still in flight before the shared
     // memory is released.
     if (tma && s_abort && i == 0) {
         for (int r = next_wait; r < issued_end; ++r) {
             const int rr = r - row0;
-            if (!mbar_wait_bounded(&mbar[rr % DI], (uint32_t)((rr / DI) & 1)))
+            if (!mbar_wait_bounded(&mbar[rr & (DI - 1)], (uint32_t)((rr / DI) & 1)))
                 break;
         }
     }

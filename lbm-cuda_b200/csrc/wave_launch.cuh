@@ -1,6 +1,8 @@
 // Host-side launcher of wave_kernel.
 #pragma once
 
+#include <stdlib.h>
+
 #include "host.h"
 #include "wave.cuh"
 
@@ -31,6 +33,12 @@ template <class C> int wave_occupancy()
 // never fewer than max(8, 2T) rows (the row halo costs 2T/chunk).
 template <class C> int default_chunk(int W, int H)
 {
+    // Tuning override for experiments: LBM_WAVE_CHUNK=<rows per CTA>.
+    if (const char *e = getenv("LBM_WAVE_CHUNK")) {
+        const int v = atoi(e);
+        if (v >= 1)
+            return v;
+    }
     const int strips = (W + C::CW - 1) / C::CW;
     const int slots = sm_count() * wave_occupancy<C>();
     int nch = slots / strips;
