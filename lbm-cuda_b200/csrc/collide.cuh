@@ -38,8 +38,12 @@ enum : int { PF_MRT = 1, PF_SMAG = 2, PF_CLAMPU = 4, PF_CLAMPF = 8, PF_INLET_SMA
 //   kClampF    the reference's population clamp f in [0, 10] (lbm_core4.cu:203,
 //              lbm_core_smemaa.cu:220)
 //   kInletSmag Smagorinsky also at the Zou-He inlet (the reference does not)
-template <bool kMrt_, bool kSmag_, bool kClampU_, bool kClampF_, bool kInletSmag_> struct Physics {
+//   kRefOrder  evaluate in the reference's order (drop-ins: rounding closest to the
+//              reference kernels); otherwise the leaner order of collide_bf
+template <bool kMrt_, bool kSmag_, bool kClampU_, bool kClampF_, bool kInletSmag_, bool kRefOrder_ = false>
+struct Physics {
     static constexpr bool kRuntime = false;
+    static constexpr bool kRefOrder = kRefOrder_;
     static constexpr bool kMrt = kMrt_;
     static constexpr bool kSmag = kSmag_;
     static constexpr bool kClampU = kClampU_;
@@ -48,9 +52,9 @@ template <bool kMrt_, bool kSmag_, bool kClampU_, bool kClampF_, bool kInletSmag
 };
 
 // lbm_core4.cu semantics: MRT + Smagorinsky, clamps, plain MRT at the inlet.
-using PhysCore4 = Physics<true, true, true, true, false>;
+using PhysCore4 = Physics<true, true, true, true, false, true>;
 // lbm_core_smemaa*.cu semantics: BGK, population clamp only.
-using PhysBgkRef = Physics<false, false, false, true, false>;
+using PhysBgkRef = Physics<false, false, false, true, false, true>;
 // General solver variants.
 using PhysMrtSmagClamp = Physics<true, true, true, true, false>; // = PhysCore4 with runtime rates and Cs
 using PhysMrtSmag = Physics<true, true, false, false, false>;
@@ -59,6 +63,7 @@ using PhysBgk = Physics<false, false, false, false, false>;
 // The same choices read from Phys::flags (uniform branches; non-hot paths).
 struct PhysRuntime {
     static constexpr bool kRuntime = true;
+    static constexpr bool kRefOrder = true;
     static constexpr bool kMrt = true, kSmag = true, kClampU = true, kClampF = true, kInletSmag = true;
 };
 
@@ -193,16 +198,23 @@ __device__ __forceinline__ void collide(float (&f)[9], bool inlet, int y, const 
     }
 }
 
-// Branch-free collision for the wavefront kernel's hot loop: the Zou-He values
-// are computed for every cell and selected where `inlet` holds (kZh = false
-// drops them at compile time for strips without the inlet column), so that the
-// scheduler can interleave the independent cells of several time levels.
-// `lu` is the inlet velocity of the cell's row.
+// Branch-free collision for the hot loops (wavefront and streaming kernels).
+// Same physics as collide() with fewer instructions:
+//   * moments from shared pair sums/differences of opposite populations;
+//   * one reciprocal of rho, square roots as x * rsqrt(x) (x > 0 here);
+//   * MRT applied as f -= M^-1 d, d = m - m' (m' the post-collision moments;
+//     for the conserved moments d0 = rho - rho', d3 = j_x - rho'u', d5 = j_y - rho'v',
+//     nonzero only when the clamps engage or at the inlet), using the structure
+//     of the Lallemand-Luo inverse (lbm_core4.cu:187-199).
+// The Zou-He values (kZh) are computed for every cell and selected where
+// `inlet` holds; `lu` is the inlet velocity of the cell's row.  Rounding
+// differs from the reference's evaluation order at the 1e-7 level.
+// Branch-free collision in the reference's evaluation order (moments summed
+// over q in sequence, MRT through the explicit moment vector).
 template <class Ph, bool kZh>
-__device__ __forceinline__ void collide_bf(float (&f)[9], bool inlet, float lu, const Phys &k, float &r, float &u,
-                                           float &v)
+__device__ __forceinline__ void collide_ref_bf(float (&f)[9], bool inlet, float lu, const Phys &k, float &r, float &u,
+                                               float &v)
 {
-    static_assert(!Ph::kRuntime, "compile-time physics only");
     moments_seq(f, r, u, v);
     if (Ph::kClampU) {
         u = fminf(0.4f, fmaxf(-0.4f, u));
@@ -232,6 +244,107 @@ __device__ __forceinline__ void collide_bf(float (&f)[9], bool inlet, float lu, 
         mrt_relax(f, r, u, v, k.s_e, k.s_eps, k.s_q, s);
     else
         bgk_relax(f, r, u, v, s);
+    if (Ph::kClampF) {
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+            f[q] = fminf(10.0f, fmaxf(0.0f, f[q]));
+    }
+}
+
+template <class Ph, bool kZh>
+__device__ __forceinline__ void collide_bf(float (&f)[9], bool inlet, float lu, const Phys &k, float &r, float &u,
+                                           float &v)
+{
+    static_assert(!Ph::kRuntime, "compile-time physics only");
+    if constexpr (Ph::kRefOrder) {
+        collide_ref_bf<Ph, kZh>(f, inlet, lu, k, r, u, v);
+        return;
+    }
+    float rz = 0.0f;
+    if (kZh) {
+        rz = (f[0] + f[2] + f[4] + 2.0f * (f[3] + f[6] + f[7])) / (1.0f - lu);
+        const float a = 0.16666666666f * rz * lu;
+        const float h = 0.5f * (f[2] - f[4]);
+        const float z1 = f[3] + 0.666666667f * rz * lu;
+        f[1] = inlet ? z1 : f[1];
+        f[5] = inlet ? f[7] - h + a : f[5];
+        f[8] = inlet ? f[6] + h + a : f[8];
+    }
+    const float a13 = f[1] + f[3], a24 = f[2] + f[4], a57 = f[5] + f[7], a68 = f[6] + f[8];
+    const float b13 = f[1] - f[3], b24 = f[2] - f[4], b57 = f[5] - f[7], b68 = f[6] - f[8];
+    const float s14 = a13 + a24, s58 = a57 + a68;
+    const float rho = (f[0] + s14) + s58;
+    const float e = b57 - b68, g = b57 + b68;
+    const float jx = b13 + e, jy = b24 + g;
+    const float rinv = __fdividef(1.0f, rho);
+    u = jx * rinv;
+    v = jy * rinv;
+    r = rho;
+    float rcinv = rinv;
+    if (Ph::kClampU) {
+        u = fminf(0.4f, fmaxf(-0.4f, u));
+        v = fminf(0.4f, fmaxf(-0.4f, v));
+        r = fminf(1.5f, fmaxf(0.0f, rho));
+        rcinv = __fdividef(1.0f, r);
+    }
+    if (kZh) {
+        r = inlet ? rz : r;
+        u = inlet ? lu : u;
+        v = inlet ? 0.0f : v;
+        rcinv = inlet ? __fdividef(1.0f, rz) : rcinv;
+    }
+    const float uu = u * u, vv = v * v;
+    const float m3 = r * u, m5 = r * v;
+    const float m7 = a13 - a24, m8 = a57 - a68;
+    const float n7 = m7 - r * (uu - vv);
+    const float n8 = m8 - m3 * v;
+    float s = k.s_nu;
+    if (Ph::kSmag) {
+        const float q2 = fmaf(n7, n7, fmaf(n8, n8, 1e-8f));
+        const float Q = q2 * rsqrtf(q2);
+        const float X = fmaf(k.cs2x18 * Q, rcinv, k.tau0 * k.tau0);
+        const float Sx = X * rsqrtf(X);
+        const float sm = __fdividef(2.0f, k.tau0 + Sx);
+        s = (kZh && inlet && !Ph::kInletSmag) ? k.s_nu : sm;
+    }
+    if (Ph::kMrt) {
+        const bool cons = Ph::kClampU || kZh; // conserved moments may be replaced
+        const float d0 = cons ? rho - r : 0.0f;
+        const float d3 = cons ? jx - m3 : 0.0f;
+        const float d5 = cons ? jy - m5 : 0.0f;
+        const float t3 = 3.0f * (uu + vv);
+        const float m1 = fmaf(2.0f, s58, -s14) - 4.0f * f[0];
+        const float m2 = fmaf(-2.0f, s14, s58) + 4.0f * f[0];
+        const float m4 = fmaf(-2.0f, b13, e);
+        const float m6 = fmaf(-2.0f, b24, g);
+        const float d1 = k.s_e * (m1 - r * (t3 - 2.0f));
+        const float d2 = k.s_eps * (m2 - r * (1.0f - t3));
+        const float d4 = k.s_q * (m4 + m3);
+        const float d6 = k.s_q * (m6 + m5);
+        const float d7 = s * n7;
+        const float d8 = s * n8;
+        const float Z = (d0 - d1 + d2) * 0.1111111111f;
+        const float A = (4.0f * d0 - d1 - 2.0f * d2) * 0.02777777778f;
+        const float D = (4.0f * d0 + 2.0f * d1 + d2) * 0.02777777778f;
+        const float Bx = (d3 - d4) * 0.16666666666f;
+        const float By = (d5 - d6) * 0.16666666666f;
+        const float Ex = (2.0f * d3 + d4) * 0.08333333333f;
+        const float Ey = (2.0f * d5 + d6) * 0.08333333333f;
+        const float AP = fmaf(0.25f, d7, A), AM = fmaf(-0.25f, d7, A);
+        const float DP = fmaf(0.25f, d8, D), DM = fmaf(-0.25f, d8, D);
+        const float EP = Ex + Ey, EM = Ex - Ey;
+        f[0] -= Z;
+        f[1] -= AP + Bx;
+        f[3] -= AP - Bx;
+        f[2] -= AM + By;
+        f[4] -= AM - By;
+        f[5] -= DP + EP;
+        f[7] -= DP - EP;
+        f[6] -= DM - EM;
+        f[8] -= DM + EM;
+    } else {
+        bgk_relax(f, r, u, v, s);
+    }
     if (Ph::kClampF) {
 #pragma unroll
         for (int q = 0; q < 9; ++q)

@@ -165,32 +165,37 @@ template <class C> __global__ void __launch_bounds__(128, 4) stream_kernel(const
     const bool xl_ok = xl >= 0 && xl < W, xr_ok = xr >= 0 && xr < W;
 
     // ---------------- round 1: every load of the step ----------------
-    uint32_t mw[3], ml[3], mr[3];
+    // Row offsets of rows y-1, y, y+1 (wrapped when periodic), computed once.
+    long long roff[3], moff[3];
+    bool rok[3];
 #pragma unroll
-    for (int dy = -1; dy <= 1; ++dy) {
-        int r = y + dy;
+    for (int d = 0; d < 3; ++d) {
+        int r = y + d - 1;
         if (pyper)
             r = wrap(r, H);
-        const bool rok = r >= 0 && r < H;
-        const uint8_t *mrow = p.mask + (long long)r * p.mask_pitch;
-        mw[dy + 1] = ldg_u32_pred(mrow + x4, rok && xok);
-        ml[dy + 1] = ldg_u8_pred(mrow + xl, rok && lane == 0 && xl_ok);
-        mr[dy + 1] = ldg_u8_pred(mrow + xr, rok && redge && xr_ok);
+        rok[d] = r >= 0 && r < H;
+        roff[d] = (long long)r * p.pitch;
+        moff[d] = (long long)r * p.mask_pitch;
+    }
+    uint32_t mw[3], ml[3], mr[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const uint8_t *mrow = p.mask + moff[d];
+        mw[d] = ldg_u32_pred(mrow + x4, rok[d] && xok);
+        ml[d] = ldg_u8_pred(mrow + xl, rok[d] && lane == 0 && xl_ok);
+        mr[d] = ldg_u8_pred(mrow + xr, rok[d] && redge && xr_ok);
     }
     V v[9];
     float edge[9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
-        int r = y - cy(q);
-        if (pyper)
-            r = wrap(r, H);
-        const bool rok = r >= 0 && r < H;
-        const E *rowp = fin + q * p.plane + (long long)r * p.pitch;
-        v[q] = ld4<E>(rowp + x4, rok && xok);
+        const int d = 1 - cy(q); // source row y - c_y
+        const E *rowp = fin + q * p.plane + roff[d];
+        v[q] = ld4<E>(rowp + x4, rok[d] && xok);
         if (cx(q) == 1)
-            edge[q] = ld1<St>(rowp + xl, rok && lane == 0 && xl_ok, q);
+            edge[q] = ld1<St>(rowp + xl, rok[d] && lane == 0 && xl_ok, q);
         else if (cx(q) == -1)
-            edge[q] = ld1<St>(rowp + xr, rok && redge && xr_ok, q);
+            edge[q] = ld1<St>(rowp + xr, rok[d] && redge && xr_ok, q);
         else
             edge[q] = 0.0f;
     }
@@ -219,22 +224,21 @@ template <class C> __global__ void __launch_bounds__(128, 4) stream_kernel(const
             f[q][3] = redge ? edge[q] : right;
         }
     }
-    // mask neighbours of the thread's cells: columns x4-1 .. x4+4, rows y-1 .. y+1
-    uint64_t win[3];
+    // mask bytes of columns x4-1 and x4+4 come from the neighbouring lanes
+    uint32_t mlx[3], mrx[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
         const uint32_t left = __shfl_up_sync(0xffffffffu, mw[d], 1) >> 24;
         const uint32_t right = __shfl_down_sync(0xffffffffu, mw[d], 1) & 0xffu;
-        const uint32_t l = lane == 0 ? ml[d] : left;
-        const uint32_t rr = redge ? mr[d] : right;
-        win[d] = (uint64_t)l | ((uint64_t)mw[d] << 8) | ((uint64_t)rr << 40);
+        mlx[d] = lane == 0 ? ml[d] : left;
+        mrx[d] = redge ? mr[d] : right;
     }
 
     // Interior cells: rows 1..H-2 (walls and periodic rows take the generic
     // path), columns 1..W-3 (no inlet, outlet source or ghost), no solid cell
     // in the 3x3 neighbourhood of any of the four cells.
-    const bool interior = xok && y >= 1 && y <= H - 2 && x4 >= 1 && x4 + 3 <= W - 3 &&
-                          ((win[0] | win[1] | win[2]) & 0xffffffffffffull) == 0;
+    const uint32_t any_solid = mw[0] | mw[1] | mw[2] | mlx[0] | mlx[1] | mlx[2] | mrx[0] | mrx[1] | mrx[2];
+    const bool interior = xok && y >= 1 && y <= H - 2 && x4 >= 1 && x4 + 3 <= W - 3 && any_solid == 0;
     const bool fast = __all_sync(0xffffffffu, interior);
 
     float out[9][4], ro[4], uo[4], vo[4];
@@ -254,6 +258,10 @@ template <class C> __global__ void __launch_bounds__(128, 4) stream_kernel(const
         }
     } else {
         // ---------------- generic path ----------------
+        uint64_t win[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+            win[d] = (uint64_t)mlx[d] | ((uint64_t)mw[d] << 8) | ((uint64_t)mrx[d] << 40);
         uint32_t code[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {

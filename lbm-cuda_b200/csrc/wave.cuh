@@ -304,14 +304,6 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
             lu_ring[slot] = inlet_u(p.k, pyper ? wrap(r, p.H) : r);
     };
 
-    // Value of level t-1 at (row rt + dr, column x + dc), population q.
-    auto src = [&](auto t_tag, int rt, int dr, int q, int dc) -> float {
-        constexpr int t = decltype(t_tag)::value;
-        if (t == 1)
-            return St::load(in_row(rt + dr)[q * RW + i + of + dc], q);
-        return lv_row(t - 1, rt + dr)[q * LW + i + 1 + dc];
-    };
-
     // ---- level computations ----
     // Level t at iteration k works on row r1 - 2(t-1).  All T levels are
     // computed in every iteration (levels outside their row range compute on
@@ -372,6 +364,25 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
             }
             const bool fast = !__any_sync(0xffffffffu, special);
 
+            // Source row pointers of every level (rows rt-1, rt, rt+1 of level t-1),
+            // already offset to this thread's column, so loads use immediate offsets.
+            const E *ib[3];
+            const float *lb[T][3];
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                ib[d] = in_row(rt[0] - 1 + d) + i + of;
+#pragma unroll
+                for (int t = 2; t <= T; ++t)
+                    lb[t - 1][d] = lv_row(t - 1, rt[t - 1] - 1 + d) + i + 1;
+            }
+            auto srcp = [&](auto t_tag, int dr, int q, int dc) -> float {
+                constexpr int t = decltype(t_tag)::value;
+                if constexpr (t == 1)
+                    return St::load(ib[dr + 1][q * RW + dc], q);
+                else
+                    return lb[t - 1][dr + 1][q * LW + dc];
+            };
+
             float f[T][9];
             float mr[T], mu[T], mv[T];
             if (fast) {
@@ -379,7 +390,7 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
                     constexpr int t = decltype(tt)::value;
 #pragma unroll
                     for (int q = 0; q < 9; ++q)
-                        f[t - 1][q] = src(tt, rt[t - 1], -cy(q), q, -cx(q));
+                        f[t - 1][q] = srcp(tt, -cy(q), q, -cx(q));
                 });
 #pragma unroll
                 for (int t = 0; t < T; ++t)
@@ -390,11 +401,11 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
                     constexpr int t = decltype(tt)::value;
 #pragma unroll
                     for (int q = 0; q < 9; ++q)
-                        own[t - 1][q] = src(tt, rt[t - 1], 0, q, 0);
+                        own[t - 1][q] = srcp(tt, 0, q, 0);
                     f[t - 1][0] = own[t - 1][0];
 #pragma unroll
                     for (int q = 1; q < 9; ++q)
-                        f[t - 1][q] = src(tt, rt[t - 1], -cy(q), q, -cx(q));
+                        f[t - 1][q] = srcp(tt, -cy(q), q, -cx(q));
                 });
 #pragma unroll
                 for (int t = 0; t < T; ++t) {
