@@ -38,33 +38,38 @@ struct AaParams {
     Phys k;
 };
 
-template <int T_, int VAR_> struct AaCfg {
+template <int T_, int VAR_, int SX_ = 64, int SY_ = 32, int NT_ = 256, int NB_ = 4, int MINB_ = 2> struct AaCfg {
     static constexpr int T = T_;
     static constexpr int VAR = VAR_;
-    static constexpr int SX = 64, SY = 32; // tile incl. halo
+    static constexpr int SX = SX_, SY = SY_; // tile incl. halo
     static constexpr int CX = SX - 2 * T, CY = SY - 2 * T;
     static constexpr int SW = SX + 4;      // smem row stride: room for the 16-byte TMA alignment offset
     static constexpr int PL = SW * SY;     // floats per population plane
     static constexpr int MW = SX + 16;     // mask row bytes (TMA box, 16-byte aligned origin)
-    static constexpr int NT = 256;
-    static constexpr int ROWS_PER_THREAD = SY / (NT / SX);
+    static constexpr int NT = NT_;
+    static constexpr int MINB = MINB_;
+    static constexpr int WPR = SX / 32;            // warps per tile row
+    static constexpr int RSTEP = NT / SX;          // rows between a thread's cells
+    static constexpr int ROWS_PER_THREAD = SY / RSTEP;
+    static_assert(SX % 32 == 0 && NT % SX == 0 && SY % RSTEP == 0, "thread map");
     static constexpr int OFF_F = 128;
     static constexpr int OFF_M = OFF_F + 9 * PL * 4;
     static constexpr int OFF_C = OFF_M + round_up(MW * SY, 128);
     static constexpr int OFF_LU = OFF_C + SX * SY * 2;
     static constexpr int OFF_DUM = OFF_LU + SY * 4;
     static constexpr int SMEM = OFF_DUM + 9 * NT * 4;
-    static constexpr int BATCH = 4;
+    static constexpr int BATCH = NB_;
+    static_assert(ROWS_PER_THREAD % NB_ == 0, "batch");
     static constexpr uint32_t TX = 9 * PL * 4 + MW * SY;
     static_assert(T % 2 == 0 && T >= 2 && CY > 0, "T");
-    static_assert(SMEM <= 113 * 1024, "two CTAs per SM");
+    static_assert(SMEM <= 227 * 1024, "shared memory");
 };
 
 // code bits: bit q (1..8) = the cell x - c_q is solid; bit 0 = cell updated.
 enum : uint16_t { AA_UPD = 1 };
 
 template <class C>
-__global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant__ AaParams p,
+__global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_constant__ AaParams p,
                                                            const __grid_constant__ CUtensorMap tmf,
                                                            const __grid_constant__ CUtensorMap tmm)
 {
@@ -77,8 +82,9 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
 
     const int W = p.W, H = p.H;
     const int tid = threadIdx.x;
-    const int col = (tid & 31) + 32 * ((tid >> 5) & 1); // 0..63
-    const int rb = tid >> 6;                           // 0..3
+    const int col = (tid & 31) + 32 * ((tid >> 5) % C::WPR); // 0..SX-1
+    const int rb = (tid >> 5) / C::WPR;                       // 0..RSTEP-1
+    constexpr int RS = C::RSTEP;
     const int xt = blockIdx.x * CX - T;                // global x of tile column 0
     const int yt = blockIdx.y * CY - T;
     const bool tma = p.use_tma != 0;
@@ -128,7 +134,7 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
     };
 #pragma unroll
     for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
-        const int r = rb + 4 * j, c = col;
+        const int r = rb + RS * j, c = col;
         const int x = xt + c, y = yt + r;
         uint16_t cd = 0;
         if (x >= 0 && x < W - 1 && y > 0 && y < H - 1 && !solid(c, r))
@@ -180,7 +186,7 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
             bool act[NB];
 #pragma unroll
             for (int jj = 0; jj < NB; ++jj) {
-                const int r = rb + 4 * (b + jj), c = col;
+                const int r = rb + RS * (b + jj), c = col;
                 act[jj] = r >= m && r < SY - m && c >= m && c < SX - m && (code[r * SX + c] & AA_UPD);
 #pragma unroll
                 for (int q = 0; q < 9; ++q)
@@ -188,13 +194,13 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
             }
 #pragma unroll
             for (int jj = 0; jj < NB; ++jj) {
-                const int r = rb + 4 * (b + jj);
+                const int r = rb + RS * (b + jj);
                 float rr, uu, vv;
                 collide_bf<PhysBgkRef, ZH>(f[jj], ZH && (xt + col == 0), ZH ? lu_row[r] : 0.0f, p.k, rr, uu, vv);
             }
 #pragma unroll
             for (int jj = 0; jj < NB; ++jj) {
-                const int r = rb + 4 * (b + jj), c = col;
+                const int r = rb + RS * (b + jj), c = col;
 #pragma unroll
                 for (int q = 0; q < 9; ++q)
                     *(act[jj] ? &sl(opp(q), c, r) : dummy + q * C::NT) = f[jj][q];
@@ -217,7 +223,7 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
             bool ok = true;
 #pragma unroll
             for (int jj = 0; jj < NB; ++jj) {
-                const int r0 = rb + 4 * (b + jj), c0 = col;
+                const int r0 = rb + RS * (b + jj), c0 = col;
                 const bool in = r0 >= m && r0 < SY - m && c0 >= m && c0 < SX - m;
                 rr_[jj] = in ? r0 : m;
                 cc_[jj] = in ? c0 : m;
@@ -257,7 +263,7 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
             }
 #pragma unroll
             for (int jj = 0; jj < NB; ++jj) {
-                const int r = rb + 4 * (b + jj);
+                const int r = rb + RS * (b + jj);
                 float r_, u_, v_;
                 collide_bf<PhysBgkRef, ZH>(f[jj], ZH && (xt + col == 0), ZH ? lu_row[r] : 0.0f, p.k, r_, u_, v_);
             }
@@ -287,7 +293,7 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
         const long long N = (long long)W * H;
 #pragma unroll
         for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
-            const int r = rb + 4 * j, c = col;
+            const int r = rb + RS * j, c = col;
             if (r < m || r >= SY - m || c < m || c >= SX - m)
                 continue;
             const uint16_t cd = code[r * SX + c];
@@ -358,7 +364,7 @@ __global__ void __launch_bounds__(C::NT, 2) aa_tile_kernel(const __grid_constant
     const long long N = (long long)W * H;
 #pragma unroll
     for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
-        const int r = rb + 4 * j, c = col;
+        const int r = rb + RS * j, c = col;
         if (r < T || r >= T + CY || c < T || c >= T + CX)
             continue;
         const int x = xt + c, y = yt + r;

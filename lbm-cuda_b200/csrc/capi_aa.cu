@@ -1,6 +1,7 @@
 // C-ABI drop-ins for the shared-memory AA kernels of the reference:
 // lbm_core_smemaa.cu (lbm_smemaa_step) and lbm_core_smemaa_policy.cu /
 // lbm_core_smemaa_endfused.cu (lbm_blocked_step).
+#include <stdlib.h>
 #include <string.h>
 
 #include "aa_tile.cuh"
@@ -36,20 +37,35 @@ template <class C> int launch_aa(AaParams p, cudaStream_t s)
     return status(cudaGetLastError());
 }
 
-template <int VAR> static int aa_dispatch(const AaParams &p, int T, cudaStream_t s)
+// Tile shapes: (SX, SY, threads, cells per batch, CTAs per SM).  Shape 0 is a
+// 64 x 32 tile (less halo recomputation), shape 1 a 32 x 32 tile with more
+// CTAs per SM (more warps to hide latency).
+template <int VAR, int SHAPE> static int aa_dispatch_shape(const AaParams &p, int T, cudaStream_t s)
 {
+    constexpr int SX = SHAPE == 0 ? 64 : 32, SY = 32, NT = SHAPE == 0 ? 256 : 256, NB = SHAPE == 0 ? 4 : 2;
+    constexpr int MB = SHAPE == 0 ? 2 : 3;
     switch (T) {
     case 2:
-        return launch_aa<AaCfg<2, VAR>>(p, s);
+        return launch_aa<AaCfg<2, VAR, SX, SY, NT, NB, MB>>(p, s);
     case 4:
-        return launch_aa<AaCfg<4, VAR>>(p, s);
+        return launch_aa<AaCfg<4, VAR, SX, SY, NT, NB, MB>>(p, s);
     case 6:
-        return launch_aa<AaCfg<6, VAR>>(p, s);
+        return launch_aa<AaCfg<6, VAR, SX, SY, NT, NB, MB>>(p, s);
     case 8:
-        return launch_aa<AaCfg<8, VAR>>(p, s);
+        return launch_aa<AaCfg<8, VAR, SX, 48, NT, NB, MB>>(p, s);
     default:
         return LBM_ERR_UNSUPPORTED;
     }
+}
+
+template <int VAR> static int aa_dispatch(const AaParams &p, int T, cudaStream_t s)
+{
+    static int shape = -1;
+    if (shape < 0) {
+        const char *e = getenv("LBM_AA_SHAPE"); // tuning override for experiments
+        shape = (e && atoi(e) == 0) ? 0 : 1;
+    }
+    return shape == 0 ? aa_dispatch_shape<VAR, 0>(p, T, s) : aa_dispatch_shape<VAR, 1>(p, T, s);
 }
 
 static AaParams aa_params(const uint8_t *mask, const float *f_now, float *f_out, float *ux, float *uy, float *rho,

@@ -244,16 +244,24 @@ template <class C> __global__ void __launch_bounds__(128, 4) stream_kernel(const
     float out[9][4], ro[4], uo[4], vo[4];
     bool wr[4];
     if (fast) {
+        float g[4][9];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                g[j][q] = f[q][j];
+        if constexpr (Ph::kRefOrder) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                collide_bf<Ph, false>(g[j], false, 0.0f, p.k, ro[j], uo[j], vo[j]);
+        } else {
+            collide_multi<Ph, 4>(g, p.k, ro, uo, vo);
+        }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            float g[9];
 #pragma unroll
             for (int q = 0; q < 9; ++q)
-                g[q] = f[q][j];
-            collide_bf<Ph, false>(g, false, 0.0f, p.k, ro[j], uo[j], vo[j]);
-#pragma unroll
-            for (int q = 0; q < 9; ++q)
-                out[q][j] = g[q];
+                out[q][j] = g[j][q];
             wr[j] = true;
         }
     } else {

@@ -392,9 +392,13 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
                     for (int q = 0; q < 9; ++q)
                         f[t - 1][q] = srcp(tt, -cy(q), q, -cx(q));
                 });
+                if constexpr (Ph::kRefOrder) {
 #pragma unroll
-                for (int t = 0; t < T; ++t)
-                    collide_bf<Ph, false>(f[t], false, 0.0f, p.k, mr[t], mu[t], mv[t]);
+                    for (int t = 0; t < T; ++t)
+                        collide_bf<Ph, false>(f[t], false, 0.0f, p.k, mr[t], mu[t], mv[t]);
+                } else {
+                    collide_multi<Ph, T>(f, p.k, mr, mu, mv);
+                }
             } else {
                 float own[T][9];
                 static_for<1, T + 1>([&](auto tt) {
