@@ -481,6 +481,93 @@ void visualize(const float *ux, const float *uy, uint8_t *img, const uint8_t *ma
         }
 }
 
+
+// ---------------------------------------------------------------------------
+// General solver step (lbm_params semantics; no reference counterpart beyond
+// the physics above).  Pull step on post-collision populations, ping-pong:
+//   * out-of-domain sources are stationary walls unless the side is periodic;
+//   * mask 0 = fluid, 2 = wall moving with (u_lid, 0) (Ladd: the bounced
+//     population gains 6 w_q rho_w c_q.u_w, rho_w = 1), other nonzero = solid;
+//   * bc_left Zou-He (flat or the reference's ramp) on the fluid cells of x = 0;
+//   * bc_right outflow: column W-1 is a ghost receiving the post-collision
+//     populations of x = W-2 (lbm_core4.cu:114-116);
+//   * cells that are not updated keep f_out's previous contents.
+// iparams = {W, H, collision(0 BGK, 1 MRT), closure(0 none, 1 Smagorinsky),
+//            bc_left, bc_right, bc_y, ref_clamps}
+// dparams = {s_nu, s_e, s_eps, s_q, cs, u_in, u_lid}
+// BC codes: 0 wall, 1 periodic, 2 Zou-He, 3 Zou-He with ramp, 4 outflow.
+// ---------------------------------------------------------------------------
+template <class S>
+void general_step(const int *ip, const double *dp, const uint8_t *mask, const S *fn, S *fo, S *ux, S *uy, S *rho)
+{
+    const int W = ip[0], H = ip[1], coll = ip[2], clos = ip[3], bl = ip[4], br = ip[5], by = ip[6], clamps = ip[7];
+    const S s_nu = S(dp[0]), s_e = S(dp[1]), s_eps = S(dp[2]), s_q = S(dp[3]), cs = S(dp[4]), u_in = S(dp[5]),
+            u_lid = S(dp[6]);
+    const bool px = bl == 1, py = by == 1, outflow = br == 4, zh = bl == 2 || bl == 3, ramp = bl == 3;
+    const long N = (long)W * H;
+    const S tau0 = S(1) / s_nu;
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y) {
+        for (int x = 0; x < W; ++x) {
+            const long pid = (long)y * W + x;
+            if (mask[pid] != 0 || (outflow && x == W - 1))
+                continue;
+            S f[9];
+            for (int q = 0; q < 9; ++q) {
+                int sx = x - CX[q], sy = y - CY[q];
+                bool out = false;
+                if (px)
+                    sx = (sx + W) % W;
+                else if (sx < 0 || sx >= W)
+                    out = true;
+                if (py)
+                    sy = (sy + H) % H;
+                else if (sy < 0 || sy >= H)
+                    out = true;
+                int mv = out ? 1 : mask[(long)sy * W + sx];
+                if (mv) {
+                    S b = fn[OPP[q] * N + pid];
+                    if (mv == 2)
+                        b += S(6) * wq<S>(q) * S(CX[q]) * u_lid;
+                    f[q] = b;
+                } else {
+                    f[q] = fn[q * N + (long)sy * W + sx];
+                }
+            }
+            S r, u, v, s = s_nu;
+            const bool inlet = zh && x == 0;
+            if (inlet) {
+                S lu = ramp ? ramp_u(u_in, y, H) : u_in;
+                r = zou_he(f, lu);
+                u = lu;
+                v = 0;
+            } else {
+                moments(f, r, u, v);
+                if (clamps) {
+                    u = clampv(u, S(-0.4), S(0.4));
+                    v = clampv(v, S(-0.4), S(0.4));
+                    r = clampv(r, S(0), S(1.5));
+                }
+                if (clos == 1)
+                    s = smag_rate(f, r, u, v, tau0, cs);
+            }
+            ux[pid] = u;
+            uy[pid] = v;
+            rho[pid] = r;
+            if (coll == 1)
+                mrt_relax(f, r, u, v, s_e, s_eps, s_q, s);
+            else
+                bgk(f, r, u, v, s);
+            for (int q = 0; q < 9; ++q) {
+                S o = clamps ? clampv(f[q], S(0), S(10)) : f[q];
+                fo[q * N + pid] = o;
+                if (outflow && x == W - 2)
+                    fo[q * N + pid + 1] = o;
+            }
+        }
+    }
+}
+
 } // namespace
 
 extern "C" {
@@ -543,6 +630,18 @@ void orc_policy_launch_f64(const uint8_t *mask, const double *fn, double *fo, in
 void orc_macro_f32(const float *f, float *ux, float *uy, float *rho, const uint8_t *mask, int W, int H, float u_in)
 {
     macro<float>(f, ux, uy, rho, mask, W, H, u_in);
+}
+
+void orc_general_step_f32(const int *ip, const double *dp, const uint8_t *mask, const float *fn, float *fo, float *ux,
+                          float *uy, float *rho)
+{
+    general_step<float>(ip, dp, mask, fn, fo, ux, uy, rho);
+}
+
+void orc_general_step_f64(const int *ip, const double *dp, const uint8_t *mask, const double *fn, double *fo,
+                          double *ux, double *uy, double *rho)
+{
+    general_step<double>(ip, dp, mask, fn, fo, ux, uy, rho);
 }
 
 void orc_visualize(const float *ux, const float *uy, uint8_t *img, const uint8_t *mask, int W, int H,

@@ -28,6 +28,8 @@ _SIGS = {
     "orc_policy_launch_f64": [_P, _P, _P, _I, _I, _D, _D, _I],
     "orc_macro_f32": [_P, _P, _P, _P, _P, _I, _I, _F],
     "orc_visualize": [_P, _P, _P, _P, _I, _I, _F],
+    "orc_general_step_f32": [_P] * 8,
+    "orc_general_step_f64": [_P] * 8,
     "orc_num_threads": [],
     "orc_set_threads": [_I],
 }
@@ -127,3 +129,35 @@ def visualize(ux, uy, mask, vort_scale=50.0, img=None):
     img = np.zeros((H, W, 4), np.uint8) if img is None else img
     lib().orc_visualize(_p(ux), _p(uy), _p(img), _p(mask), W, H, vort_scale)
     return img
+
+
+BC = {"wall": 0, "periodic": 1, "zouhe": 2, "zouhe_ramp": 3, "outflow": 4}
+
+
+class General:
+    """Parameters of the general solver step (lbm_params semantics)."""
+
+    def __init__(self, W, H, collision="mrt", closure="smag", s_nu=1.8, s_e=1.1, s_eps=1.1, s_q=1.1, cs=0.2,
+                 bc_left="zouhe_ramp", bc_right="outflow", bc_y="wall", u_in=0.1, u_lid=0.0, ref_clamps=True):
+        self.ip = np.array([W, H, 1 if collision == "mrt" else 0, 1 if closure == "smag" else 0, BC[bc_left],
+                            BC[bc_right], BC[bc_y], int(bool(ref_clamps))], dtype=np.int32)
+        self.dp = np.array([s_nu, s_e, s_eps, s_q, cs, u_in, u_lid], dtype=np.float64)
+
+    def step(self, mask, f_now, f_out=None, macro=None):
+        _, H, W = f_now.shape
+        f_out = f_now.copy() if f_out is None else f_out
+        if macro is None:
+            macro = tuple(np.zeros((H, W), dtype=f_now.dtype) for _ in range(3))
+        fn = getattr(lib(), "orc_general_step_" + _dt(f_now))
+        fn(_p(self.ip), _p(self.dp), _p(mask), _p(f_now), _p(f_out), _p(macro[0]), _p(macro[1]), _p(macro[2]))
+        return f_out, macro
+
+    def run(self, mask, f0, n_steps, macro=None):
+        a, b = f0.copy(), f0.copy()
+        _, H, W = f0.shape
+        if macro is None:
+            macro = tuple(np.zeros((H, W), dtype=f0.dtype) for _ in range(3))
+        for _ in range(n_steps):
+            self.step(mask, a, b, macro)
+            a, b = b, a
+        return a, macro
