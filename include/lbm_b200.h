@@ -159,6 +159,42 @@ int lbm_forces_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d
 /* Convert a state between storage formats (W*H*9 elements each). */
 int lbm_convert_state(int W, int H, const void *src, int src_storage, void *dst, int dst_storage, void *stream);
 
+/* ------------------------------------------------------------------------
+ * Batched independent domains (no reference counterpart): many domains of
+ * uneven size advance together in one persistent launch per T steps; the
+ * CTAs take (domain, strip, row-chunk) work items from a device counter.
+ * ------------------------------------------------------------------------ */
+
+typedef struct lbm_domain {
+    int W, H;
+    int pitch;       /* elements between rows of a plane (0 = W); multiples of 16 enable TMA */
+    int mask_pitch;  /* bytes between mask rows (0 = W) */
+    void *f_a, *f_b; /* ping-pong states, 9 planes of pitch*H elements of the batch's storage */
+    const uint8_t *mask;
+    float u_in;      /* inlet velocity of this domain */
+} lbm_domain;
+
+typedef struct lbm_batch lbm_batch;
+
+/* Copies the domain table (and a per-domain tensor-map table) to the device.
+ * common->W/H are ignored; the physics variant must be MRT + Smagorinsky
+ * with FP32 or FP16-deviation storage. */
+int lbm_batch_create(const lbm_params *common, const lbm_domain *domains, int n, lbm_batch **out);
+int lbm_batch_destroy(lbm_batch *b);
+
+/* n_steps steps of every domain, T per launch (T = 0: the autotuned choice,
+ * else 1..8).  Launch pairs are replayed from a captured CUDA graph unless the
+ * stream is itself capturing.  *result_in_b = 1 when the states end in f_b. */
+int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in_b);
+
+/* The same steps with one ordinary launch per domain (the comparison point). */
+int lbm_batch_run_separate(lbm_batch *b, int n_steps, int T, void *stream, int *result_in_b);
+
+/* Time candidate (T, rows per work item) pairs on the batch and keep the fastest
+ * for T = 0.  Advances every domain by an even number of steps per candidate
+ * (states end in f_a).  Synchronous. */
+int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk);
+
 /* Read (and optionally clear) the device error word of the current device:
  * bit 0 = a bounded device-side wait gave up.  Synchronises the device. */
 int lbm_device_error_flags(int *flags, int clear);

@@ -1,0 +1,453 @@
+// Batched independent domains: one persistent launch advances every domain T
+// steps.  CTAs (sm_count x occupancy of them) take (domain, strip, row-chunk)
+// work items from a device counter and run the wavefront tile of wave.cuh on
+// each, so domains of uneven size share the GPU without one launch per domain.
+// Launch pairs (ping-pong) are captured once into a CUDA graph and replayed.
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "dispatch.cuh"
+
+namespace lbm {
+
+struct __align__(64) BatchDomain {
+    CUtensorMap tmf[2]; // input map when f_a (0) / f_b (1) is the source
+    CUtensorMap tmm;
+    WaveParams p;
+    void *f[2];
+};
+
+constexpr int kBatchNX = 128;
+
+template <class C> struct BatchSmem {
+    static constexpr int OFF_PRM = round_up(C::SMEM, 16);
+    static constexpr int OFF_ITEM = OFF_PRM + round_up((int)sizeof(WaveParams), 16);
+    static constexpr int SMEM = OFF_ITEM + 16;
+};
+
+template <class C>
+__global__ void __launch_bounds__(C::NX, C::MINB)
+    batch_kernel(const BatchDomain *__restrict__ doms, const int4 *__restrict__ items, int n_items, int *counter,
+                 int parity)
+{
+    extern __shared__ __align__(128) unsigned char smem[];
+    WaveParams *sp = reinterpret_cast<WaveParams *>(smem + BatchSmem<C>::OFF_PRM);
+    volatile int *s_item = reinterpret_cast<volatile int *>(smem + BatchSmem<C>::OFF_ITEM);
+    bool first = true;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0)
+            *s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = *s_item;
+        if (it >= n_items)
+            break;
+        const int4 item = items[it];
+        const BatchDomain &d = doms[item.x];
+        if (threadIdx.x == 0) {
+            WaveParams w = d.p;
+            w.f_in = d.f[parity];
+            w.f_out = d.f[parity ^ 1];
+            *sp = w;
+        }
+        __syncthreads();
+        wave_tile<C>(*sp, &d.tmf[parity], &d.tmm, item.y, item.z, !first);
+        first = false;
+    }
+}
+
+template <class Ph, class St, int T> using BCfg = WaveCfg<T, kBatchNX, Ph, St, MODE_GENERAL>;
+
+// Resident CTAs per SM of a batch configuration (also raises the smem limit).
+template <class C> static int batch_occupancy()
+{
+    const int smem = BatchSmem<C>::SMEM;
+    cudaFuncSetAttribute(batch_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, batch_kernel<C>, C::NX, smem);
+    return n < 1 ? 1 : n;
+}
+
+template <class C>
+static int batch_launch(const BatchDomain *d, const int4 *items, int n_items, int *counter, int parity,
+                        cudaStream_t s)
+{
+    const int grid = sm_count() * batch_occupancy<C>();
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), s);
+    if (e != cudaSuccess)
+        return status(e);
+    batch_kernel<C><<<grid, C::NX, BatchSmem<C>::SMEM, s>>>(d, items, n_items, counter, parity);
+    return status(cudaGetLastError());
+}
+
+// Dispatch on (clamps, storage, T).
+template <template <class> class F, class... A> static int with_cfg(int clamps, int storage, int T, A &&...a)
+{
+    auto go = [&](auto ph, auto st) -> int {
+        using Ph = decltype(ph);
+        using St = decltype(st);
+        switch (T) {
+        case 1:
+            return F<BCfg<Ph, St, 1>>::run(a...);
+        case 2:
+            return F<BCfg<Ph, St, 2>>::run(a...);
+        case 4:
+            return F<BCfg<Ph, St, 4>>::run(a...);
+        case 8:
+            return F<BCfg<Ph, St, 8>>::run(a...);
+        default:
+            return LBM_ERR_UNSUPPORTED;
+        }
+    };
+    if (storage == LBM_STORE_F32)
+        return clamps ? go(PhysMrtSmagClamp{}, StoreF32{}) : go(PhysMrtSmag{}, StoreF32{});
+    if (storage == LBM_STORE_F16DEV)
+        return clamps ? go(PhysMrtSmagClamp{}, StoreF16Dev{}) : go(PhysMrtSmag{}, StoreF16Dev{});
+    return LBM_ERR_UNSUPPORTED;
+}
+
+template <class C> struct LaunchOp {
+    static int run(const BatchDomain *d, const int4 *items, int n_items, int *counter, int parity, cudaStream_t s)
+    {
+        return batch_launch<C>(d, items, n_items, counter, parity, s);
+    }
+};
+template <class C> struct CwOp {
+    static int run(int *cw)
+    {
+        *cw = C::CW;
+        return LBM_OK;
+    }
+};
+template <class C> struct RwOp {
+    static int run(int *rw, int *rwm)
+    {
+        *rw = C::RW;
+        *rwm = C::RWM;
+        return LBM_OK;
+    }
+};
+template <class C> struct SeparateOp {
+    static int run(const WaveParams &p, cudaStream_t s)
+    {
+        return launch_wave<C>(p, s);
+    }
+};
+
+} // namespace lbm
+
+using namespace lbm;
+
+struct lbm_batch {
+    lbm_params p;
+    std::vector<lbm_domain> doms;
+    std::vector<BatchDomain> hdoms;
+    BatchDomain *d_doms = nullptr;
+    int4 *d_items = nullptr;
+    int max_items = 0;
+    int n_items = 0;
+    int *d_counter = nullptr;
+    int cur_T = 0, cur_chunk = 0; // configuration the device item list holds
+    std::vector<int4> h_items;
+    int tuned_T = 4, tuned_chunk = 64;
+    cudaStream_t cap = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int exec_T = 0, exec_chunk = 0;
+};
+
+static int batch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
+{
+    if (b->cur_T == T && b->cur_chunk == chunk)
+        return LBM_OK;
+    int cw = 0;
+    int rc = with_cfg<CwOp>(b->p.ref_clamps, b->p.storage, T, &cw);
+    if (rc)
+        return rc;
+    b->h_items.clear();
+    for (int d = 0; d < (int)b->doms.size(); ++d) {
+        const int strips = (b->doms[d].W + cw - 1) / cw;
+        const int chunks = (b->doms[d].H + chunk - 1) / chunk;
+        for (int by = 0; by < chunks; ++by)
+            for (int bx = 0; bx < strips; ++bx)
+                b->h_items.push_back(make_int4(d, bx, by, 0));
+    }
+    if ((int)b->h_items.size() > b->max_items)
+        return LBM_ERR_ARG;
+    for (auto &hd : b->hdoms)
+        hd.p.chunk = chunk;
+    cudaError_t e = cudaMemcpyAsync(b->d_items, b->h_items.data(), sizeof(int4) * b->h_items.size(),
+                                    cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_doms, b->hdoms.data(), sizeof(BatchDomain) * b->hdoms.size(),
+                            cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s); // the host vectors may change before the copies run otherwise
+    if (e != cudaSuccess)
+        return status(e);
+    b->n_items = (int)b->h_items.size();
+    b->cur_T = T;
+    b->cur_chunk = chunk;
+    return LBM_OK;
+}
+
+static int batch_launch_one(lbm_batch *b, int T, int parity, cudaStream_t s)
+{
+    return with_cfg<LaunchOp>(b->p.ref_clamps, b->p.storage, T, (const BatchDomain *)b->d_doms,
+                              (const int4 *)b->d_items, b->n_items, b->d_counter, parity, s);
+}
+
+extern "C" {
+
+int lbm_batch_create(const lbm_params *common, const lbm_domain *domains, int n, lbm_batch **out)
+{
+    if (!common || !domains || n < 1 || !out)
+        return LBM_ERR_ARG;
+    *out = nullptr;
+    if (common->collision != LBM_COLL_MRT || common->closure != LBM_CLOSURE_SMAG || common->u_lid != 0.0f ||
+        (common->storage != LBM_STORE_F32 && common->storage != LBM_STORE_F16DEV))
+        return LBM_ERR_UNSUPPORTED;
+    if ((common->bc_left == LBM_BC_PERIODIC) != (common->bc_right == LBM_BC_PERIODIC))
+        return LBM_ERR_ARG;
+    lbm_batch *b = new lbm_batch();
+    b->p = *common;
+    b->doms.assign(domains, domains + n);
+    const int es = common->storage == LBM_STORE_F32 ? 4 : 2;
+    int rw = 0, rwm = 0;
+    with_cfg<RwOp>(common->ref_clamps, common->storage, 4, &rw, &rwm);
+    b->hdoms.resize(n);
+    int max_items = 0;
+    for (int d = 0; d < n; ++d) {
+        lbm_domain dm = domains[d];
+        if (dm.W < 3 || dm.H < 3 || !dm.f_a || !dm.f_b || !dm.mask || dm.f_a == dm.f_b) {
+            delete b;
+            return LBM_ERR_ARG;
+        }
+        if (!dm.pitch)
+            dm.pitch = dm.W;
+        if (!dm.mask_pitch)
+            dm.mask_pitch = dm.W;
+        b->doms[d] = dm;
+        BatchDomain &hd = b->hdoms[d];
+        memset(&hd, 0, sizeof(hd));
+        WaveParams &w = hd.p;
+        w.mask = dm.mask;
+        w.W = dm.W;
+        w.H = dm.H;
+        w.pitch = dm.pitch;
+        w.plane = (long long)dm.pitch * dm.H;
+        w.mask_pitch = dm.mask_pitch;
+        w.bc_left = common->bc_left;
+        w.bc_right = common->bc_right;
+        w.bc_y = common->bc_y;
+        w.err = device_error_word();
+        w.k.s_nu = common->s_nu;
+        w.k.s_e = common->s_e;
+        w.k.s_eps = common->s_eps;
+        w.k.s_q = common->s_q;
+        w.k.tau0 = 1.0f / common->s_nu;
+        w.k.cs2x18 = 18.0f * common->cs_smag * common->cs_smag;
+        w.k.u_in = dm.u_in;
+        w.k.H = dm.H;
+        w.k.ramp = common->bc_left == LBM_BC_ZOUHE_RAMP;
+        hd.f[0] = dm.f_a;
+        hd.f[1] = dm.f_b;
+        bool tma = common->bc_left != LBM_BC_PERIODIC && aligned16(dm.f_a) && aligned16(dm.f_b) &&
+                   aligned16(dm.mask) && ((long long)dm.pitch * es) % 16 == 0 && (w.plane * es) % 16 == 0 &&
+                   dm.mask_pitch % 16 == 0;
+        if (tma)
+            tma = make_map_planes(&hd.tmf[0], dm.f_a, es, dm.W, dm.H, dm.pitch, w.plane, rw) &&
+                  make_map_planes(&hd.tmf[1], dm.f_b, es, dm.W, dm.H, dm.pitch, w.plane, rw) &&
+                  make_map_mask(&hd.tmm, dm.mask, dm.W, dm.H, dm.mask_pitch, rwm);
+        w.use_tma = tma ? 1 : 0;
+        // bound on the work items of any (T, chunk >= 8) configuration
+        max_items += ((dm.W + (kBatchNX - 16) - 1) / (kBatchNX - 16)) * ((dm.H + 7) / 8);
+    }
+    b->max_items = max_items;
+    cudaError_t e = cudaMalloc(&b->d_doms, sizeof(BatchDomain) * n);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_items, sizeof(int4) * max_items);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->d_counter, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        lbm_batch_destroy(b);
+        return status(e);
+    }
+    *out = b;
+    return LBM_OK;
+}
+
+int lbm_batch_destroy(lbm_batch *b)
+{
+    if (!b)
+        return LBM_ERR_ARG;
+    if (b->exec)
+        cudaGraphExecDestroy(b->exec);
+    if (b->cap)
+        cudaStreamDestroy(b->cap);
+    cudaFree(b->d_doms);
+    cudaFree(b->d_items);
+    cudaFree(b->d_counter);
+    delete b;
+    return LBM_OK;
+}
+
+int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in_b)
+{
+    if (!b || n_steps < 0 || T < 0 || T > 8)
+        return LBM_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int chunk = b->tuned_chunk;
+    if (T == 0)
+        T = b->tuned_T;
+    if (T != 1 && T != 2 && T != 4 && T != 8)
+        return LBM_ERR_UNSUPPORTED;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(s, &cs);
+    const bool capturing = cs != cudaStreamCaptureStatusNone;
+    if (!(b->cur_T == T && b->cur_chunk == chunk)) {
+        if (capturing)
+            return LBM_ERR_ARG; // the item list must be prepared outside a capture (run once first)
+        int rc = batch_items(b, T, chunk, s);
+        if (rc)
+            return rc;
+    }
+    int done = 0, parity = 0;
+    const int pairs = n_steps / (2 * T);
+    if (pairs > 0 && !capturing) {
+        if (!b->exec || b->exec_T != T || b->exec_chunk != chunk) {
+            if (b->exec) {
+                cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+            }
+            cudaGraph_t g = nullptr;
+            cudaError_t e = cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess)
+                return status(e);
+            int rc = batch_launch_one(b, T, 0, b->cap);
+            if (!rc)
+                rc = batch_launch_one(b, T, 1, b->cap);
+            e = cudaStreamEndCapture(b->cap, &g);
+            if (rc || e != cudaSuccess) {
+                if (g)
+                    cudaGraphDestroy(g);
+                return rc ? rc : status(e);
+            }
+            e = cudaGraphInstantiate(&b->exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess)
+                return status(e);
+            b->exec_T = T;
+            b->exec_chunk = chunk;
+        }
+        for (int i = 0; i < pairs; ++i) {
+            cudaError_t e = cudaGraphLaunch(b->exec, s);
+            if (e != cudaSuccess)
+                return status(e);
+        }
+        done = pairs * 2 * T;
+    }
+    while (done < n_steps) {
+        // remaining steps: launches of depth T, then the largest supported depth that fits
+        const int left = n_steps - done;
+        const int t = left >= T ? T : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
+        if (t != b->cur_T) {
+            if (capturing)
+                return LBM_ERR_ARG;
+            int rc = batch_items(b, t, chunk, s);
+            if (rc)
+                return rc;
+        }
+        int rc = batch_launch_one(b, t, parity, s);
+        if (rc)
+            return rc;
+        done += t;
+        parity ^= 1;
+    }
+    if (result_in_b)
+        *result_in_b = parity;
+    return LBM_OK;
+}
+
+int lbm_batch_run_separate(lbm_batch *b, int n_steps, int T, void *stream, int *result_in_b)
+{
+    if (!b || n_steps < 0 || T < 1 || T > 8)
+        return LBM_ERR_ARG;
+    if (T != 1 && T != 2 && T != 4 && T != 8)
+        return LBM_ERR_UNSUPPORTED;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int parity = 0;
+    for (int done = 0; done < n_steps;) {
+        const int t = (n_steps - done >= T) ? T : ((n_steps - done) >= 4 ? 4 : ((n_steps - done) >= 2 ? 2 : 1));
+        for (size_t d = 0; d < b->hdoms.size(); ++d) {
+            WaveParams w = b->hdoms[d].p;
+            w.f_in = b->hdoms[d].f[parity];
+            w.f_out = b->hdoms[d].f[parity ^ 1];
+            w.chunk = 0;
+            int rc = with_cfg<SeparateOp>(b->p.ref_clamps, b->p.storage, t, w, s);
+            if (rc)
+                return rc;
+        }
+        done += t;
+        parity ^= 1;
+    }
+    if (result_in_b)
+        *result_in_b = parity;
+    return LBM_OK;
+}
+
+int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk)
+{
+    if (!b)
+        return LBM_ERR_ARG;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int Ts[] = {1, 2, 4, 8};
+    const int chunks[] = {16, 32, 64, 128};
+    float best = 1e30f;
+    int bT = 4, bC = 64;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    for (int T : Ts) {
+        for (int ch : chunks) {
+            if (ch < 2 * T)
+                continue;
+            int rc = batch_items(b, T, ch, s);
+            if (rc)
+                return rc;
+            for (int w = 0; w < 2; ++w)
+                if ((rc = batch_launch_one(b, T, w & 1, s)))
+                    return rc;
+            cudaEventRecord(e0, s);
+            for (int w = 0; w < 4; ++w)
+                if ((rc = batch_launch_one(b, T, w & 1, s)))
+                    return rc;
+            cudaEventRecord(e1, s);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess)
+                return status(e);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            const float per_step = ms / (4.0f * T);
+            if (per_step < best) {
+                best = per_step;
+                bT = T;
+                bC = ch;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->tuned_T = bT;
+    b->tuned_chunk = bC;
+    if (best_T)
+        *best_T = bT;
+    if (best_chunk)
+        *best_chunk = bC;
+    return LBM_OK;
+}
+
+} // extern "C"

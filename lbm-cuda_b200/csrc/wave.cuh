@@ -186,10 +186,11 @@ __device__ __forceinline__ uint32_t build_code_general(const Nbhd &n, int x, int
     return c;
 }
 
+// One tile (strip bx, chunk by) of the wavefront.  `reinit` re-initialises the
+// mbarriers of a CTA that already ran a tile (persistent batch kernel).
 template <class C>
-__global__ void __launch_bounds__(C::NX, C::MINB)
-    wave_kernel(const __grid_constant__ WaveParams p, const __grid_constant__ CUtensorMap tmf,
-                const __grid_constant__ CUtensorMap tmm)
+__device__ __forceinline__ void wave_tile(const WaveParams &p, const CUtensorMap *tmf, const CUtensorMap *tmm, int bx,
+                                          int by, bool reinit)
 {
     using St = typename C::St;
     using E = typename C::E;
@@ -206,10 +207,10 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
     volatile int &s_abort = *reinterpret_cast<int *>(smem + C::OFF_BAR + 124);
 
     const int i = threadIdx.x;
-    const int x0 = blockIdx.x * CW;
+    const int x0 = bx * CW;
     const int xs = x0 - T;
     const int x = xs + i;
-    const int ya = blockIdx.y * p.chunk;
+    const int ya = by * p.chunk;
     const int yb = min(p.H, ya + p.chunk);
     const int row0 = ya - T;
     const int nin = yb - ya + 2 * T;
@@ -231,11 +232,14 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
     if (i == 0) {
         s_abort = 0;
         if (tma) {
-            for (int s = 0; s < DI; ++s)
+            for (int s = 0; s < DI; ++s) {
+                if (reinit)
+                    mbar_inval(&mbar[s]);
                 mbar_init(&mbar[s], 1);
+            }
             mbar_fence_init();
-            prefetch_tmap(&tmf);
-            prefetch_tmap(&tmm);
+            prefetch_tmap(tmf);
+            prefetch_tmap(tmm);
         }
     }
     for (int j = i; j < C::NLV * 4 * 9 * LW; j += NX)
@@ -246,8 +250,8 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
         const int s = (r - row0) & (DI - 1);
         const int ry = pyper ? wrap(r, p.H) : r;
         mbar_arrive_expect_tx(&mbar[s], C::TX_BYTES);
-        tma_load_3d(in_base + s * C::SLOT_F, &tmf, &mbar[s], xf0, ry, 0);
-        tma_load_2d(m_base + s * C::SLOT_M, &tmm, &mbar[s], xm0, ry);
+        tma_load_3d(in_base + s * C::SLOT_F, tmf, &mbar[s], xf0, ry, 0);
+        tma_load_2d(m_base + s * C::SLOT_M, tmm, &mbar[s], xm0, ry);
     };
     // Plain path: thread i loads ring entries i and (i < 2) NX + i, i.e. columns
     // xs - 1 + e; out-of-range columns/rows read zero unless periodic.
@@ -484,6 +488,14 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
                 break;
         }
     }
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::NX, C::MINB)
+    wave_kernel(const __grid_constant__ WaveParams p, const __grid_constant__ CUtensorMap tmf,
+                const __grid_constant__ CUtensorMap tmm)
+{
+    wave_tile<C>(p, &tmf, &tmm, blockIdx.x, blockIdx.y, false);
 }
 
 } // namespace lbm

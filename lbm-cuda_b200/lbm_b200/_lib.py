@@ -31,6 +31,11 @@ SIGNATURES = {
     "lbm_forces_fp64": ([_P] * 4 + [_P], _I),
     "lbm_convert_state": ([_I, _I, _P, _I, _P, _I, _P], _I),
     "lbm_device_error_flags": ([_IP, _I], _I),
+    "lbm_batch_create": ([_P, _P, _I, C.POINTER(C.c_void_p)], _I),
+    "lbm_batch_destroy": ([_P], _I),
+    "lbm_batch_run": ([_P, _I, _I, _P, _IP], _I),
+    "lbm_batch_run_separate": ([_P, _I, _I, _P, _IP], _I),
+    "lbm_batch_autotune": ([_P, _P, _IP, _IP], _I),
     "lbm_error_string": ([_I], C.c_char_p),
     "lbm_version": ([], _I),
 }
