@@ -31,6 +31,7 @@ extern "C" {
 #define LBM_ERR_UNSUPPORTED 1002 /* configuration not built (e.g. temporal depth T) */
 #define LBM_ERR_DEVICE 1003      /* no usable sm_100 device or driver entry point */
 #define LBM_ERR_TIMEOUT 1004     /* a bounded device-side wait gave up */
+#define LBM_ERR_TOO_LARGE 1005   /* domain larger than lbm_diag_fp64_noalloc's fixed scratch */
 
 /* Storage formats of the population planes (general solver). */
 #define LBM_STORE_F32 0
@@ -150,6 +151,20 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
  * accumulated in FP64 with a fixed-order two-pass reduction (deterministic).
  * d_out: 3 doubles of device memory. */
 int lbm_diag_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d_out, void *stream);
+
+/* lbm_diag_fp64 without a handle and without allocating: no counterpart in the
+ * reference.  For callers that cannot call cudaMalloc (a host whose allocator
+ * owns the device heap, a time loop that must not make a call that can
+ * synchronise or run out of memory, a foreign runtime that only lends its own
+ * buffers).  Its scratch is a fixed array of about 384 KiB inside the library,
+ * one per device; domains of more than LBM_NOALLOC_MAX_CELLS cells return
+ * LBM_ERR_TOO_LARGE.  The first call on a device looks up that array's address
+ * (make it before any stream capture).  All calls on a device share the array:
+ * calls whose work overlaps on the GPU race and must be ordered by the caller.
+ * f: W*H*9 elements of `storage`; d_out: 3 doubles (mass, jx, jy). */
+#define LBM_NOALLOC_MAX_CELLS 134217728LL /* 16384 blocks x 8192 cells, e.g. 16384 x 8192 */
+int lbm_diag_fp64_noalloc(int W, int H, int storage, const void *f, const uint8_t *mask, double *d_out,
+                          void *stream);
 
 /* Momentum-exchange force on LBM_MASK_OBSTACLE cells, sum 2 c_q f_q(x) over fluid
  * x and directions q with x + c_q an obstacle cell, in FP64 (deterministic).

@@ -202,6 +202,8 @@ const char *lbm_error_string(int st)
         return "no usable sm_100 device";
     case LBM_ERR_TIMEOUT:
         return "a bounded device-side wait gave up";
+    case LBM_ERR_TOO_LARGE:
+        return "domain exceeds the fixed scratch of lbm_diag_fp64_noalloc (LBM_NOALLOC_MAX_CELLS cells)";
     default:
         return (st > 0 && st < 1000) ? cudaGetErrorString(static_cast<cudaError_t>(st)) : "unknown status";
     }

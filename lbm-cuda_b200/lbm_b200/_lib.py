@@ -29,6 +29,7 @@ SIGNATURES = {
     "lbm_run": ([_P] * 4 + [_I, _I, _P, _P, _P, _P, _IP], _I),
     "lbm_diag_fp64": ([_P] * 4 + [_P], _I),
     "lbm_forces_fp64": ([_P] * 4 + [_P], _I),
+    "lbm_diag_fp64_noalloc": ([_I, _I, _I, _P, _P, _P, _P], _I),
     "lbm_convert_state": ([_I, _I, _P, _I, _P, _I, _P], _I),
     "lbm_device_error_flags": ([_IP, _I], _I),
     "lbm_batch_create": ([_P, _P, _I, C.POINTER(C.c_void_p)], _I),
