@@ -5,14 +5,20 @@ Workload (the channel-flow-past-a-cylinder configuration): 4096 x 1024 D2Q9,
 MRT + Smagorinsky (Cs = 0.1), FP32, Zou-He velocity inlet u = 0.05 (cosine
 ramp as in the reference), zero-gradient outlet, bounce-back channel walls,
 cylinder D = 128 centred at (1024, 512), nu = 6.4e-4 (tau = 0.50192),
-initial u_y noise uniform +-1e-4 from numpy PCG64 seed 0, T = 4 steps fused
-per launch.  Synthetic inputs with that shape (there is no external dataset).
+initial u_y noise uniform +-1e-4 from numpy PCG64 seed 0.  --T sets the
+steps fused per launch (default 1, the streaming kernel, which is the fastest
+path for this workload today; 2-8 run the temporally blocked kernel).
+Synthetic inputs with that shape (there is no external dataset).
 
-One bench "step" is one frame of `--frame` physical steps (default 100 =
-25 launches of T = 4).  Metric: MLUPS = W*H*physical steps / time, counting
-every cell as the reference does (lbm_mine2.py:106).
+One bench "step" is one frame of `--frame` physical steps (default 100).
+Metric: MLUPS = W*H*physical steps / time, counting every cell as the
+reference does (lbm_mine2.py:106).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--T 1..8] [--storage f32|f16|bf16] [--workload cylinder|batch]
+
+--workload batch times 256 independent channel domains of uneven size in one
+persistent launch per T steps (FP16 storage) against one launch per domain.
 
 --impl reference times the reference's own kernel for this path
 (fused_lbmkernel of lbm_core4.cu, MRT + Smagorinsky, one step per launch,
@@ -75,6 +81,7 @@ class ClockSampler:
         self.index = index
         self.proc = None
         self.lines = []
+        self.start = 0
 
     def __enter__(self):
         try:
@@ -83,6 +90,10 @@ class ClockSampler:
                  "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            t0 = time.time()  # the timed region starts once the sampler is producing
+            while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.01)
+            self.start = len(self.lines)
         except (OSError, FileNotFoundError):
             self.proc = None
         return self
@@ -102,7 +113,10 @@ class ClockSampler:
     def summary(self):
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        # samples taken inside the timed region; the last one before it when the
+        # region was shorter than the sampling period
+        lines = self.lines[self.start:] or self.lines[-1:]
+        for ln in lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 8:
                 continue
@@ -155,9 +169,13 @@ def main():
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--T", type=int, default=4, help="steps fused per launch (ours)")
+    ap.add_argument("--T", type=int, default=1,
+                    help="steps fused per launch (1: streaming kernel; 2-8: wavefront temporal blocking)")
     ap.add_argument("--frame", type=int, default=100, help="physical steps per bench step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32",
+                    help="population storage of the cylinder workload (16-bit: deviations f - w)")
+    ap.add_argument("--workload", choices=["cylinder", "batch"], default="cylinder")
     args = ap.parse_args()
 
     rank, world, local = dist_env()
@@ -193,13 +211,26 @@ def main():
         return
 
     import lbm_b200 as L
+    from lbm_b200 import solver as SV
     from lbm_b200.solver import Solver
 
+    if args.workload == "batch":
+        line = run_batch(args, torch, rank, world, barrier, max_over_ranks)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if world > 1:
+            barrier()
+            dist.destroy_process_group()
+        return
+
+    storage = {"f32": SV.STORE_F32, "f16": SV.STORE_F16DEV, "bf16": SV.STORE_BF16DEV}[args.storage]
+    b_alg = B_ALG if storage == SV.STORE_F32 else B_ALG / 2
     mask_np, f0_np = workload()
     mask = torch.from_numpy(mask_np).cuda()
-    f_a = torch.from_numpy(f0_np).cuda()
+    S = Solver(W, H, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU, storage=storage)
+    f_a = torch.empty((9, H, W), dtype=S.dtype, device="cuda")
+    SV.convert_state(torch.from_numpy(f0_np).cuda(), SV.STORE_F32, f_a, storage)
     f_b = f_a.clone()
-    S = Solver(W, H, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU)
     T = args.T
     n_launch = (args.frame + T - 1) // T
     stream = torch.cuda.current_stream()
@@ -235,7 +266,7 @@ def main():
     # End to end through the public API with host buffers: every step uploads
     # the state and mask from pinned host memory, runs the frame and reads back
     # u, v, rho of the last step.
-    host_f = torch.from_numpy(f0_np).pin_memory()
+    host_f = f_a.cpu().pin_memory()
     host_m = torch.from_numpy(mask_np).pin_memory()
     host_mac = [torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in range(3)]
     dev_mac = [torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in range(3)]
@@ -270,9 +301,11 @@ def main():
     flags = L.solver.device_error_flags(clear=True)
     if rank == 0:
         peak, peak_src = hbm_peak()
-        achieved = B_ALG * W * H * T / (launch_ms * 1e-3) / 1e9
+        achieved = b_alg * W * H * T / (launch_ms * 1e-3) / 1e9
         traffic = None
-        tfile = os.path.join(ROOT, "profiles", "wave_kernel_T4_4096x1024_traffic.json")
+        kname = "stream_kernel" if T == 1 else "wave_kernel"
+        suffix = "" if args.storage == "f32" else "_" + args.storage
+        tfile = os.path.join(ROOT, "profiles", f"{kname}_T{T}_{W}x{H}{suffix}_traffic.json")
         if os.path.exists(tfile):
             try:
                 traffic = json.load(open(tfile))["dram_bytes_per_launch"]
@@ -285,6 +318,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": f"cylinder channel {W}x{H} D2Q9 MRT+Smagorinsky Cs={CS}, Zou-He u={U_IN}, "
                                    f"D={CYL[2]} at ({CYL[0]},{CYL[1]}), nu={NU}, T={T} steps per launch",
+                       "storage": args.storage,
                        "W": W, "H": H, "T": T, "physical_steps_per_step": n_launch * T,
                        "l2": "inputs larger than L2 (two 151 MB population buffers)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
@@ -292,18 +326,82 @@ def main():
                     "d2h_bytes_per_step": int(d2h)},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "kernel": "wave_kernel (MRT+Smagorinsky, T steps per launch)",
-                         "note": f"achieved = 72 B per lattice update x W*H*T / launch time; peak {peak_src}"},
+                         "kernel": f"{kname} (MRT+Smagorinsky, {T} step(s) per launch)",
+                         "note": f"achieved = {b_alg:g} B per lattice update x W*H*T / launch time; "
+                                 f"peak {peak_src}"},
             "gpu_launches": args.steps * n_launch,
             "clocks": clk.summary(),
             "device_error_flags": flags,
         }
-        if not args.no_cpu_baseline and world == 1:
+        if not args.no_cpu_baseline and world == 1 and storage == SV.STORE_F32:
             line["cpu_baseline"] = cpu_baseline()
         print(json.dumps(line), flush=True)
     if world > 1:
         barrier()
         dist.destroy_process_group()
+
+
+def run_batch(args, torch, rank, world, barrier, max_over_ranks):
+    """256 independent MRT+Smagorinsky channel domains, Nx, Ny ~ U[64, 1024], 1-4
+    discs of radius 4-32, inlet u ~ U[0.02, 0.08], FP16-deviation storage, one
+    persistent launch per T steps (autotuned T and rows per work item), against
+    one launch per domain."""
+    from lbm_b200 import init as I
+    from lbm_b200 import solver as SV
+    from lbm_b200.batch import Batch
+
+    rng = np.random.default_rng(1234 + rank)
+    doms = []
+    cells = 0
+    for i in range(256):
+        w, h = int(rng.integers(64, 1025)), int(rng.integers(64, 1025))
+        m = I.random_discs_mask(w, h, int(rng.integers(1, 5)), 4.0, min(32.0, h / 4), 5000 + i)
+        pitch = (w + 15) // 16 * 16
+        mk = torch.zeros((h, pitch), dtype=torch.uint8, device="cuda")
+        mk[:, :w] = torch.from_numpy(m).cuda()
+        fa = torch.zeros((9, h, pitch), dtype=torch.float16, device="cuda")  # deviation 0: fluid at rest
+        doms.append(dict(W=w, H=h, pitch=pitch, mask_pitch=pitch, f_a=fa, f_b=fa.clone(), mask=mk,
+                         u_in=float(rng.uniform(0.02, 0.08))))
+        cells += w * h
+    B = Batch(doms, storage=SV.STORE_F16DEV, cs_smag=CS, s_nu=1.0 / TAU)
+    T, chunk = B.autotune()
+    steps_per = 40
+    stream = torch.cuda.current_stream()
+    for _ in range(args.warmup):
+        B.run(steps_per, T)
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            B.run(steps_per, T)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    mlups = cells * steps_per * args.steps * world / (ms * 1e3)
+    B.run_separate(steps_per, T)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(max(1, args.steps // 3)):
+        B.run_separate(steps_per, T)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_sep = max_over_ranks(e0.elapsed_time(e1))
+    mlups_sep = cells * steps_per * max(1, args.steps // 3) * world / (ms_sep * 1e3)
+    return {
+        "metric": "aggregate MLUPS", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f16-deviation storage, f32 math",
+        "data": "synthetic",
+        "config": {"workload": "batch of 256 MRT+Smagorinsky channel domains, Nx,Ny~U[64,1024], 1-4 discs r 4-32, "
+                               "u_in~U[0.02,0.08], FP16 storage, persistent launch, autotuned",
+                   "cells": cells, "T": T, "rows_per_item": chunk, "physical_steps_per_step": steps_per},
+        "separate_launches_mlups": round(mlups_sep, 1),
+        "speedup_vs_separate": round(mlups / mlups_sep, 3),
+        "gpu_launches": args.steps * ((steps_per + T - 1) // T),
+        "clocks": clk.summary(),
+    }
 
 
 def run_reference(args, torch):
