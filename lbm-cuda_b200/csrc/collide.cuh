@@ -503,4 +503,148 @@ __device__ __forceinline__ void collide_multi(float (&f)[N][9], const Phys &k, f
     }
 }
 
+// ---------------------------------------------------------------------------
+// Two cells at once on Blackwell's packed FP32 pipe (FFMA2 / FADD2 / FMUL2:
+// one instruction updates both halves of a float2, each half rounded as the
+// scalar operation would be).  Same physics and evaluation order as
+// collide_multi; reciprocals and square roots stay scalar.  The reference's
+// clamps are applied only when a value is outside its range: the check works
+// on the IEEE bit patterns (for x >= +0, bits(x) <= bits(hi) <=> x <= hi;
+// negative values, -0 and NaN compare above every positive bound), so a value
+// inside the range is returned unchanged and any other value goes through the
+// same fminf / fmaxf as before -- the result equals the unconditional clamp.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 bc2(float s)
+{
+    return make_float2(s, s);
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+    return __fadd2_rn(a, b);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) // a - b, one rounding
+{
+    return __ffma2_rn(b, make_float2(-1.0f, -1.0f), a);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b)
+{
+    return __fmul2_rn(a, b);
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c)
+{
+    return __ffma2_rn(a, b, c);
+}
+__device__ __forceinline__ float2 rcp2(float2 a)
+{
+    return make_float2(__fdividef(1.0f, a.x), __fdividef(1.0f, a.y));
+}
+__device__ __forceinline__ float2 rsqrt2(float2 a)
+{
+    return make_float2(rsqrtf(a.x), rsqrtf(a.y));
+}
+__device__ __forceinline__ uint32_t fbits(float x)
+{
+    return __float_as_uint(x);
+}
+
+template <class Ph>
+__device__ __forceinline__ void collide_pair(float2 (&f)[9], const Phys &k, float2 &r, float2 &u, float2 &v)
+{
+    static_assert(!Ph::kRuntime && !Ph::kRefOrder, "fast-order compile-time physics only");
+    const float2 a13 = add2(f[1], f[3]), a24 = add2(f[2], f[4]), a57 = add2(f[5], f[7]), a68 = add2(f[6], f[8]);
+    const float2 b13 = sub2(f[1], f[3]), b24 = sub2(f[2], f[4]), b57 = sub2(f[5], f[7]), b68 = sub2(f[6], f[8]);
+    const float2 s14 = add2(a13, a24), s58 = add2(a57, a68);
+    const float2 rho = add2(add2(f[0], s14), s58);
+    const float2 e = sub2(b57, b68), g = add2(b57, b68);
+    const float2 jx = add2(b13, e), jy = add2(b24, g);
+    const float2 rinv = rcp2(rho);
+    u = mul2(jx, rinv);
+    v = mul2(jy, rinv);
+    r = rho;
+    float2 rcinv = rinv;
+    if (Ph::kClampU) {
+        const uint32_t mu = max(max(fbits(u.x) & 0x7fffffffu, fbits(u.y) & 0x7fffffffu),
+                                max(fbits(v.x) & 0x7fffffffu, fbits(v.y) & 0x7fffffffu));
+        const uint32_t mr = max(fbits(r.x), fbits(r.y));
+        if (mu > fbits(0.4f) || mr > fbits(1.5f)) {
+            u.x = fminf(0.4f, fmaxf(-0.4f, u.x));
+            u.y = fminf(0.4f, fmaxf(-0.4f, u.y));
+            v.x = fminf(0.4f, fmaxf(-0.4f, v.x));
+            v.y = fminf(0.4f, fmaxf(-0.4f, v.y));
+            r.x = fminf(1.5f, fmaxf(0.0f, rho.x));
+            r.y = fminf(1.5f, fmaxf(0.0f, rho.y));
+            rcinv = rcp2(r);
+        }
+    }
+    const float2 uu = mul2(u, u), vv = mul2(v, v);
+    const float2 m3 = mul2(r, u), m5 = mul2(r, v);
+    const float2 n7 = fma2(r, sub2(vv, uu), sub2(a13, a24));
+    const float2 n8 = sub2(sub2(a57, a68), mul2(m3, v));
+    float2 s = bc2(k.s_nu);
+    if (Ph::kSmag) {
+        const float2 q2 = fma2(n7, n7, fma2(n8, n8, bc2(1e-8f)));
+        const float2 Q = mul2(q2, rsqrt2(q2));
+        const float2 X = fma2(mul2(bc2(k.cs2x18), Q), rcinv, bc2(k.tau0 * k.tau0));
+        const float2 Sx = mul2(X, rsqrt2(X));
+        s = mul2(bc2(2.0f), rcp2(add2(bc2(k.tau0), Sx)));
+    }
+    if (Ph::kMrt) {
+        float2 d0 = bc2(0.0f), d3 = bc2(0.0f), d5 = bc2(0.0f);
+        if (Ph::kClampU) {
+            d0 = sub2(rho, r);
+            d3 = sub2(jx, m3);
+            d5 = sub2(jy, m5);
+        }
+        const float2 t3 = mul2(bc2(3.0f), add2(uu, vv));
+        const float2 m1 = fma2(bc2(-4.0f), f[0], sub2(add2(s58, s58), s14));
+        const float2 m2 = fma2(bc2(4.0f), f[0], fma2(bc2(-2.0f), s14, s58));
+        const float2 d1 = mul2(bc2(k.s_e), fma2(r, sub2(bc2(2.0f), t3), m1));
+        const float2 d2 = mul2(bc2(k.s_eps), fma2(r, add2(t3, bc2(-1.0f)), m2));
+        const float2 d4 = mul2(bc2(k.s_q), add2(fma2(bc2(-2.0f), b13, e), m3));
+        const float2 d6 = mul2(bc2(k.s_q), add2(fma2(bc2(-2.0f), b24, g), m5));
+        const float2 d7 = mul2(s, n7), d8 = mul2(s, n8);
+        const float2 Z = mul2(add2(sub2(d0, d1), d2), bc2(0.1111111111f));
+        const float2 A = mul2(fma2(bc2(4.0f), d0, fma2(bc2(-2.0f), d2, mul2(d1, bc2(-1.0f)))), bc2(0.02777777778f));
+        const float2 D = mul2(fma2(bc2(4.0f), d0, fma2(bc2(2.0f), d1, d2)), bc2(0.02777777778f));
+        const float2 Bx = mul2(sub2(d3, d4), bc2(0.16666666666f));
+        const float2 By = mul2(sub2(d5, d6), bc2(0.16666666666f));
+        const float2 Ex = mul2(fma2(bc2(2.0f), d3, d4), bc2(0.08333333333f));
+        const float2 Ey = mul2(fma2(bc2(2.0f), d5, d6), bc2(0.08333333333f));
+        const float2 AP = fma2(bc2(0.25f), d7, A), AM = fma2(bc2(-0.25f), d7, A);
+        const float2 DP = fma2(bc2(0.25f), d8, D), DM = fma2(bc2(-0.25f), d8, D);
+        const float2 EP = add2(Ex, Ey), EM = sub2(Ex, Ey);
+        f[0] = sub2(f[0], Z);
+        f[1] = sub2(f[1], add2(AP, Bx));
+        f[3] = sub2(f[3], sub2(AP, Bx));
+        f[2] = sub2(f[2], add2(AM, By));
+        f[4] = sub2(f[4], sub2(AM, By));
+        f[5] = sub2(f[5], add2(DP, EP));
+        f[7] = sub2(f[7], sub2(DP, EP));
+        f[6] = sub2(f[6], sub2(DM, EM));
+        f[8] = sub2(f[8], add2(DM, EM));
+    } else {
+        const float2 usq = add2(uu, vv);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const float2 cu = fma2(bc2((float)cx(q)), u, mul2(bc2((float)cy(q)), v));
+            const float2 poly = fma2(mul2(bc2(4.5f), cu), cu, fma2(bc2(3.0f), cu, fma2(bc2(-1.5f), usq, bc2(1.0f))));
+            const float2 feq = mul2(mul2(bc2(wgt(q)), r), poly);
+            f[q] = fma2(s, sub2(feq, f[q]), f[q]);
+        }
+    }
+    if (Ph::kClampF) {
+        uint32_t mx = 0u;
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+            mx = max(mx, max(fbits(f[q].x), fbits(f[q].y)));
+        if (mx > fbits(10.0f)) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                f[q].x = fminf(10.0f, fmaxf(0.0f, f[q].x));
+                f[q].y = fminf(10.0f, fmaxf(0.0f, f[q].y));
+            }
+        }
+    }
+}
+
 } // namespace lbm

@@ -1,7 +1,9 @@
 // Kernel selection for one launch of T fused steps: the 128-bit streaming
-// kernel for aligned single steps, the wavefront kernel otherwise.
+// kernel for aligned single steps, the register wavefront kernel for
+// TMA-aligned even T <= 6, the shared-memory wavefront kernel otherwise.
 #pragma once
 
+#include "rwave.cuh"
 #include "stream.cuh"
 #include "wave_launch.cuh"
 
@@ -35,6 +37,13 @@ int launch_step(const WaveParams &p, int T, cudaStream_t s)
 {
     if (T == 1 && stream_ok(p))
         return launch_stream<StreamCfg<Ph, St, MODE, LID>>(p, s);
+    if (rwave_ok<typename St::T>(p, T, MODE)) {
+        if (T == 2)
+            return launch_rwave<RwCfg<2, 1, 1, Ph, St, MODE, LID, true>>(p, s);
+        if (T == 4)
+            return launch_rwave<RwCfg<4, 1, 2, Ph, St, MODE, LID, false>>(p, s);
+        return launch_rwave<RwCfg<6, 1, 2, Ph, St, MODE, LID, false>>(p, s);
+    }
     switch (T) {
     case 1:
         return launch_wave<WaveCfg<1, 224, Ph, St, MODE, LID>>(p, s);

@@ -63,7 +63,7 @@ def case_inputs(kind, W, H, seed=1):
     return m, f0
 
 
-@pytest.mark.parametrize("T", [1, 2, 4, 8])
+@pytest.mark.parametrize("T", [1, 2, 4, 6, 8])
 @pytest.mark.parametrize("W,H", [(130, 66), (256, 96)])
 @pytest.mark.parametrize("name", list(CASES))
 def test_general_vs_oracle(name, W, H, T):
@@ -196,3 +196,45 @@ def test_storage_formats_error():
     if os.path.isdir(out):
         with open(os.path.join(out, "storage_errors.json"), "w") as fh:
             json.dump(errs, fh, indent=1)
+
+
+@pytest.mark.parametrize("storage", [SV.STORE_F32, SV.STORE_F16DEV])
+@pytest.mark.parametrize("T", [2, 4, 6])
+@pytest.mark.parametrize("name", ["mrt_smag_clamps_ramp", "cavity_lid", "mrt_periodic_y_channel"])
+def test_register_wavefront_matches_smem_wavefront(name, T, storage):
+    """The register wavefront kernel (TMA-aligned planes, even T) against the
+    shared-memory wavefront kernel (LBM_KERNEL=wave) and the oracle, on a domain
+    of several windows and row chunks."""
+    if name == "cavity_lid" and storage != SV.STORE_F32:
+        pytest.skip("the moving-wall variant is built for FP32 storage only")
+    W, H = 600, 264
+    kw, kind = CASES[name]
+    m, f0 = case_inputs(kind, W, H, seed=3)
+    tdt = {SV.STORE_F32: torch.float32, SV.STORE_F16DEV: torch.float16}[storage]
+    n = 2 * T + 1
+    outs = []
+    for kernel in ("", "wave"):
+        os.environ["LBM_KERNEL"] = kernel
+        try:
+            S, G = make(W, H, storage=storage, **kw)
+            a = torch.empty((9, H, W), dtype=tdt, device="cuda")
+            SV.convert_state(dev(f0), SV.STORE_F32, a, storage)
+            b = a.clone()
+            mac = [torch.zeros((H, W), device="cuda") for _ in range(3)]
+            which = S.run(a, b, dev(m), n, T, *mac)
+            f32 = torch.empty((9, H, W), dtype=torch.float32, device="cuda")
+            SV.convert_state(b if which else a, storage, f32, SV.STORE_F32)
+            outs.append((host(f32), [host(x) for x in mac]))
+        finally:
+            os.environ.pop("LBM_KERNEL", None)
+    (fr, mr), (fw, mw) = outs
+    # same arithmetic in two kernels: a few ulps (of the storage format)
+    assert rel_l2(fr, fw) < (1e-6 if storage == SV.STORE_F32 else REL_TOL)
+    upd = m == 0
+    for g_, w_ in zip(mr, mw):
+        assert rel_l2(g_[upd], w_[upd]) < (1e-6 if storage == SV.STORE_F32 else 1e-4)
+    if storage == SV.STORE_F32:
+        ref, rmac = G.run(m, f0, n)
+        assert rel_l2(fr, ref) < REL_TOL
+        for g_, r_ in zip(mr, rmac):
+            assert rel_l2(g_[upd], r_[upd]) < REL_TOL
