@@ -20,6 +20,10 @@ reference does (lbm_mine2.py:106).
 
 --workload batch times 256 independent channel domains of uneven size in one
 persistent launch per T steps (FP16 storage) against one launch per domain.
+--workload dropins times the drop-in entry points for the reference's three
+kernels (lbm_smemaa_step T=4, lbm_blocked_step T=6, lbm_core4_step) and the
+general solver's BGK path at the drivers' 2048 x 512 and at 4096 x 1024; with
+--impl reference, the reference's own kernels on the same inputs.
 
 --impl reference times the reference's own kernel for this path
 (fused_lbmkernel of lbm_core4.cu, MRT + Smagorinsky, one step per launch,
@@ -177,7 +181,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32",
                     help="population storage of the cylinder workload (16-bit: deviations f - w)")
-    ap.add_argument("--workload", choices=["cylinder", "batch"], default="cylinder")
+    ap.add_argument("--workload", choices=["cylinder", "batch", "dropins"], default="cylinder")
     args = ap.parse_args()
 
     rank, world, local = dist_env()
@@ -205,7 +209,7 @@ def main():
             if world > 1:
                 dist.destroy_process_group()
             return
-        line = run_reference(args, torch)
+        line = run_dropins(args, torch, True) if args.workload == "dropins" else run_reference(args, torch)
         print(json.dumps(line), flush=True)
         if world > 1:
             barrier()
@@ -216,8 +220,11 @@ def main():
     from lbm_b200 import solver as SV
     from lbm_b200.solver import Solver
 
-    if args.workload == "batch":
-        line = run_batch(args, torch, rank, world, barrier, max_over_ranks)
+    if args.workload in ("batch", "dropins"):
+        if args.workload == "batch":
+            line = run_batch(args, torch, rank, world, barrier, max_over_ranks)
+        else:
+            line = run_dropins(args, torch, False)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if world > 1:
@@ -413,6 +420,85 @@ def run_batch(args, torch, rank, world, barrier, max_over_ranks):
         "gpu_launches": args.steps * ((steps_per + T - 1) // T),
         "clocks": clk.summary(),
     }
+
+
+def run_dropins(args, torch, ref):
+    """Drop-in kernels (ours or, with ref, the reference's compiled from source)
+    on a channel with a solid cylinder, about 100 physical steps per size."""
+    from lbm_b200 import init as I
+
+    P, I_, F = C.c_void_p, C.c_int, C.c_float
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    libs = {}
+    if ref:
+        for name in ("core4", "smemaa", "policy", "endfused"):
+            path = os.path.join(ROOT, "oracle", "_ref", f"libref_{name}.so")
+            if not os.path.exists(path):
+                return {"impl": "reference", "unavailable": f"oracle/_ref/libref_{name}.so was not built"}
+            libs[name] = C.CDLL(path)
+        libs["core4"].ref_core4_step.argtypes = [P] * 6 + [I_, I_, F, F, F, P]
+        libs["smemaa"].ref_smemaa_step.argtypes = [P] * 6 + [I_, I_, F, F, P]
+        for name in ("policy", "endfused"):
+            libs[name].ref_blocked_step.argtypes = [P] * 3 + [I_, I_, F, F, P]
+    else:
+        import lbm_b200 as L
+        from lbm_b200 import solver as SV
+    res = {}
+    for (w, h) in ((2048, 512), (4096, 1024)):
+        m = I.cylinder_mask(w, h, w // 4, h // 2, h // 8, value=I.SOLID)
+        f0 = I.channel_state(w, h, u0=0.0, noise=1e-4, seed=0)
+        mask = torch.from_numpy(m).cuda()
+        st = {"a": torch.from_numpy(f0).cuda()}
+        st["b"] = st["a"].clone()
+        mac = [torch.zeros((h, w), dtype=torch.float32, device="cuda") for _ in range(3)]
+        if ref:
+            kern = [("smemaa_T4", int(libs["smemaa"].ref_T()), lambda a, b: libs["smemaa"].ref_smemaa_step(
+                        ptr(mask), ptr(a), ptr(b), *[ptr(t) for t in mac], w, h, 1.7, 0.1, sp)),
+                    ("policy_T6", int(libs["policy"].ref_T()), lambda a, b: libs["policy"].ref_blocked_step(
+                        ptr(mask), ptr(a), ptr(b), w, h, 1.7, 0.1, sp)),
+                    ("endfused_T6", int(libs["endfused"].ref_T()), lambda a, b: libs["endfused"].ref_blocked_step(
+                        ptr(mask), ptr(a), ptr(b), w, h, 1.7, 0.1, sp)),
+                    ("core4_T1", 1, lambda a, b: libs["core4"].ref_core4_step(
+                        ptr(mask), ptr(a), ptr(b), *[ptr(t) for t in mac], w, h, 1.7, 0.1, 1.7, sp))]
+        else:
+            S = SV.Solver(w, h, collision=SV.COLL_BGK, closure=SV.CLOSURE_NONE, ref_clamps=0, s_nu=1.7, u_in=0.1)
+            kern = [("smemaa_T4", 4, lambda a, b: L.smemaa_step(mask, a, b, *mac, w, h, 1.7, 0.1, T=4)),
+                    ("endfused_T6", 6, lambda a, b: L.blocked_step(mask, a, b, w, h, 1.7, 0.1, T=6)),
+                    ("core4_T1", 1, lambda a, b: L.core4_step(mask, a, b, *mac, w, h, 1.7, 0.1)),
+                    ("general_bgk_T2", 2, lambda a, b: S.run(a, b, mask, 2, 2)),
+                    ("general_bgk_T4", 4, lambda a, b: S.run(a, b, mask, 4, 4))]
+        for name, T, fn in kern:
+            n = max(1, 100 // T)
+
+            def go():
+                for _ in range(n):
+                    rc = fn(st["a"], st["b"])
+                    if ref and rc:
+                        raise RuntimeError(f"reference launch failed: {rc}")
+                    st["a"], st["b"] = st["b"], st["a"]
+
+            for _ in range(max(1, args.warmup)):
+                go()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                go()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            res[f"{name}_{w}x{h}"] = round(w * h * T * n * args.steps / (ms * 1e3), 1)
+    line = {"metric": "MLUPS", "value": res["smemaa_T4_2048x512"], "unit": "MLUPS", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "drop-in kernels, BGK tau_inv 1.7, u_in 0.1, channel with a solid cylinder "
+                                   "(D = H/4 at (W/4, H/2)), about 100 physical steps per bench step"},
+            "results": res}
+    if ref:
+        line["impl"] = "reference"
+    return line
 
 
 def run_reference(args, torch):
