@@ -167,6 +167,9 @@ static int variant_of(const lbm_params &p)
         v = (p.u_lid != 0.0f) ? VAR_MRT_LID : VAR_MRT;
     else if (p.collision == LBM_COLL_BGK && p.closure == LBM_CLOSURE_NONE && !p.ref_clamps && p.u_lid == 0.0f)
         v = VAR_BGK;
+    else if (p.collision == LBM_COLL_MRT && p.closure == LBM_CLOSURE_MLP && !p.ref_clamps && p.u_lid == 0.0f &&
+             p.mlp != nullptr)
+        return VAR_MRT_MLP;
     if (p.storage != LBM_STORE_F32 && (v == VAR_MRT_LID || v == VAR_BGK))
         v = -1;
     return v;
@@ -182,8 +185,10 @@ static int validate(const lbm_params *p)
         return LBM_ERR_ARG;
     if (p->collision != LBM_COLL_BGK && p->collision != LBM_COLL_MRT)
         return LBM_ERR_ARG;
-    if (p->closure != LBM_CLOSURE_NONE && p->closure != LBM_CLOSURE_SMAG)
+    if (p->closure != LBM_CLOSURE_NONE && p->closure != LBM_CLOSURE_SMAG && p->closure != LBM_CLOSURE_MLP)
         return LBM_ERR_UNSUPPORTED;
+    if (p->closure == LBM_CLOSURE_MLP && (!p->mlp || (reinterpret_cast<uintptr_t>(p->mlp) & 15u) != 0))
+        return LBM_ERR_ARG;
     if (!(p->s_nu > 0.0f && p->s_nu < 2.0f))
         return LBM_ERR_ARG;
     const int l = p->bc_left, r = p->bc_right, y = p->bc_y;
@@ -214,6 +219,7 @@ static Phys make_phys(const lbm_params &p)
     k.u_lid = p.u_lid;
     k.H = p.H;
     k.ramp = p.bc_left == LBM_BC_ZOUHE_RAMP;
+    k.mlp = p.closure == LBM_CLOSURE_MLP ? p.mlp : nullptr;
     k.flags = (p.collision == LBM_COLL_MRT ? PF_MRT : 0) | (p.closure == LBM_CLOSURE_SMAG ? PF_SMAG : 0) |
               (p.ref_clamps ? (PF_CLAMPU | PF_CLAMPF) : 0);
     return k;
@@ -338,7 +344,9 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
         wp.use_tma = 1;
         wp.k = h->k;
         int rc = LBM_ERR_ARG;
-        if (h->p.storage == LBM_STORE_F32)
+        if (h->variant == VAR_MRT_MLP)
+            rc = general_launch_mlp(h->p.storage, wp, t, s);
+        else if (h->p.storage == LBM_STORE_F32)
             rc = general_launch_f32(h->variant, wp, t, s);
         else if (h->p.storage == LBM_STORE_F16DEV)
             rc = general_launch_f16(h->variant, wp, t, s);

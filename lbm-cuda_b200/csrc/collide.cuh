@@ -26,6 +26,7 @@ struct Phys {
     int H;        // domain height (ramp profile)
     int ramp;     // 1: cosine-ramped inlet profile (reference), 0: flat
     int flags;    // PF_* (used by PhysRuntime only)
+    const void *mlp; // packed MLP weights (Physics::kMlp)
 };
 
 enum : int { PF_MRT = 1, PF_SMAG = 2, PF_CLAMPU = 4, PF_CLAMPF = 8, PF_INLET_SMAG = 16 };
@@ -40,9 +41,11 @@ enum : int { PF_MRT = 1, PF_SMAG = 2, PF_CLAMPU = 4, PF_CLAMPF = 8, PF_INLET_SMA
 //   kInletSmag Smagorinsky also at the Zou-He inlet (the reference does not)
 //   kRefOrder  evaluate in the reference's order (drop-ins: rounding closest to the
 //              reference kernels); otherwise the leaner order of collide_bf
-template <bool kMrt_, bool kSmag_, bool kClampU_, bool kClampF_, bool kInletSmag_, bool kRefOrder_ = false>
+template <bool kMrt_, bool kSmag_, bool kClampU_, bool kClampF_, bool kInletSmag_, bool kRefOrder_ = false,
+          bool kMlp_ = false>
 struct Physics {
     static constexpr bool kRuntime = false;
+    static constexpr bool kMlp = kMlp_; // learned eddy viscosity in place of Smagorinsky
     static constexpr bool kRefOrder = kRefOrder_;
     static constexpr bool kMrt = kMrt_;
     static constexpr bool kSmag = kSmag_;
@@ -60,9 +63,11 @@ using PhysMrtSmagClamp = Physics<true, true, true, true, false>; // = PhysCore4 
 using PhysMrtSmag = Physics<true, true, false, false, false>;
 using PhysMrt = Physics<true, false, false, false, false>;
 using PhysBgk = Physics<false, false, false, false, false>;
+using PhysMrtMlp = Physics<true, false, false, false, false, false, true>; // MRT + learned closure
 // The same choices read from Phys::flags (uniform branches; non-hot paths).
 struct PhysRuntime {
     static constexpr bool kRuntime = true;
+    static constexpr bool kMlp = false;
     static constexpr bool kRefOrder = true;
     static constexpr bool kMrt = true, kSmag = true, kClampU = true, kClampF = true, kInletSmag = true;
 };

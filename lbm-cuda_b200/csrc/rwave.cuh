@@ -37,6 +37,7 @@
 // the inlet or outlet column).
 #pragma once
 
+#include "mlp.cuh"
 #include "wave_launch.cuh"
 
 namespace lbm {
@@ -48,7 +49,10 @@ struct RwCfg {
     static constexpr int NW = NW_; // warps (windows) per CTA
     static constexpr int P = P_;   // TMA prefetch distance in rows
     static constexpr int D = P + 3; // ring depth: rows yk-2, yk-1, yk in use + P in flight
-    static constexpr int CW = 64 - 2 * T;
+    // Left pad of the window: T rounded up to even, so that a lane's column pair
+    // stays 8-byte aligned; CW output columns [PADL, 64 - PADL).
+    static constexpr int PADL = T_ + (T_ & 1);
+    static constexpr int CW = 64 - 2 * PADL;
     static constexpr int MODE = MODE_;
     static constexpr bool LID = LID_;
     // two-cell collision on the packed FP32x2 pipe (collide_pair) or scalar (collide_multi)
@@ -63,15 +67,17 @@ struct RwCfg {
     static constexpr int SLOT_F = round_up(9 * BW * ES, 128);
     static constexpr int SLOT = SLOT_F + 128;
     static constexpr int CR = 8; // code ring rows
-    static constexpr int WARP_BYTES = 128 + D * SLOT + CR * 32 * 8;
+    static constexpr bool MLP = Ph_::kMlp;
+    static constexpr int MLP_BYTES = MLP ? 64 * 8 * 2 + 64 * 4 : 0; // feature stage + outputs
+    static constexpr int WARP_BYTES = 128 + D * SLOT + CR * 32 * 8 + MLP_BYTES;
     static constexpr int SMEM = NW * WARP_BYTES;
     static constexpr uint32_t TX_BYTES = 9 * BW * ES + BWM;
     // resident warps per SM the registers are sized for: 16 / 12 / 8 (<= 128 / 170 / 255 registers)
-    static constexpr int MINB_R = ((T <= 2) ? 16 : ((T <= 4) ? 12 : 8)) / NW;
+    static constexpr int MINB_R = ((T <= 2 && !MLP) ? 16 : ((T <= 4) ? 12 : 8)) / NW;
     static constexpr int MINB_S = (227 * 1024) / (SMEM + 1024);
     static constexpr int MINB_A = MINB_ > 0 ? MINB_ : MINB_R; // blocks per SM the registers are sized for
     static constexpr int MINB = MINB_A < MINB_S ? MINB_A : MINB_S;
-    static_assert(T % 2 == 0 && T >= 2 && T <= 6 && CR >= T, "temporal depth");
+    static_assert(T >= 1 && T <= 6 && CR >= T, "temporal depth");
     static_assert(D * 8 <= 128, "mbarriers");
     static_assert(MINB >= 1, "shared memory");
 };
@@ -233,12 +239,12 @@ __host__ __device__ __forceinline__ void codes_from_bytes(const uint32_t (&raw)[
 struct RwItems {
     int nwin, wr, nedge, che, nche, nch, n_edge_items, n_items;
 };
-__host__ __device__ __forceinline__ RwItems rw_items(int W, int H, int CW, int T, int chunk)
+__host__ __device__ __forceinline__ RwItems rw_items(int W, int H, int CW, int PADL, int chunk)
 {
     RwItems it;
     it.nwin = (W + CW - 1) / CW;
-    // first window whose columns reach W - 3 (xs + 63 >= W - 3)
-    int wr = (W - 66 + T + CW - 1) / CW;
+    // first window whose columns reach W - 3 (xs + 63 >= W - 3, xs = w CW - PADL)
+    int wr = (W - 66 + PADL + CW - 1) / CW;
     if (wr < 1)
         wr = 1;
     if (wr > it.nwin)
@@ -268,12 +274,24 @@ __host__ __device__ __forceinline__ void rw_item(const RwItems &it, int item, in
     }
 }
 
-// Collision of a lane's two cells without Zou-He: packed or scalar.
+// Per-warp state of the learned closure (unused by the other variants).
+struct MlpCtx {
+    MlpFrag F;
+    __nv_bfloat16 *stage;
+    float *zbuf;
+    int lane;
+};
+
+// Collision of a lane's two cells without Zou-He: packed or scalar, or with the
+// learned closure (warp-collective).
 template <class C>
-__device__ __forceinline__ void collide_two(float2 (&g)[9], const Phys &k, float2 &r, float2 &u, float2 &v)
+__device__ __forceinline__ void collide_two(float2 (&g)[9], const Phys &k, float2 &r, float2 &u, float2 &v,
+                                            const MlpCtx &mc)
 {
     using Ph = typename C::Ph;
-    if constexpr (C::PACKED) {
+    if constexpr (C::MLP) {
+        collide_pair_mlp<Ph, false>(g, false, false, 0.0f, k, mc.F, mc.stage, mc.zbuf, mc.lane, r, u, v);
+    } else if constexpr (C::PACKED) {
         collide_pair<Ph>(g, k, r, u, v);
     } else {
         float f[2][9], r_[2], u_[2], v_[2];
@@ -312,7 +330,7 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wi = threadIdx.x >> 5;
-    const RwItems items = rw_items(p.W, p.H, C::CW, C::T, p.chunk);
+    const RwItems items = rw_items(p.W, p.H, C::CW, C::PADL, p.chunk);
     const int item = blockIdx.x * C::NW + wi;
     if (item >= items.n_items)
         return; // whole warp: no item left (nothing below waits on other warps)
@@ -323,8 +341,16 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
     uint64_t *bar = reinterpret_cast<uint64_t *>(wbase);
     unsigned char *ring = wbase + 128;
     uint2 *cring = reinterpret_cast<uint2 *>(wbase + 128 + D * C::SLOT);
+    MlpCtx mc;
+    mc.lane = lane;
+    if constexpr (C::MLP) {
+        unsigned char *mb = wbase + 128 + D * C::SLOT + CR * 32 * 8;
+        mc.stage = reinterpret_cast<__nv_bfloat16 *>(mb);
+        mc.zbuf = reinterpret_cast<float *>(mb + 64 * 8 * 2);
+        mlp_load_frag(static_cast<const MlpPacked *>(p.k.mlp), mc.F, lane);
+    }
 
-    const int xs = win * C::CW - T;
+    const int xs = win * C::CW - C::PADL;
     const int x = xs + 2 * lane; // column of the lane's first cell
     const int row0 = ya - T;
     const int nrows = yb - ya + 2 * T;
@@ -335,7 +361,7 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
     const int offm = (xs - xm) + 2 * lane; // byte offset of the lane's mask pair
     // Columns at or next to the domain's left/right ends are always special.
     const bool colspec = x <= 0 || x + 1 >= p.W - 2;
-    const bool core0 = 2 * lane >= T && 2 * lane < 64 - T;
+    const bool core0 = 2 * lane >= C::PADL && 2 * lane < 64 - C::PADL;
     // Window-wide work of the generic body: Zou-He inlet and outlet ghost.
     const bool win_inlet =
         xs <= 0 && (C::MODE == MODE_CORE4 || p.bc_left == LBM_BC_ZOUHE || p.bc_left == LBM_BC_ZOUHE_RAMP);
@@ -374,9 +400,10 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
 
     // Carried levels 1..T-1: pv = row yk-t-1 (all q), p2 = row yk-t-2 (q 2,5,6
     // stored at their own indices; the others unused), cu = row yk-t.
-    float2 pv[T - 1][9], p2[T - 1][9], cu[T - 1][9];
+    constexpr int NL = T > 1 ? T - 1 : 1; // carried levels (one unused slot at T = 1)
+    float2 pv[NL][9], p2[NL][9], cu[NL][9];
 #pragma unroll
-    for (int t = 0; t < T - 1; ++t)
+    for (int t = 0; t < NL; ++t)
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
             pv[t][q] = make_float2(wgt(q), wgt(q));
@@ -460,7 +487,7 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
             pull2(S, O, N, g);
             float2 r_, u_, v_;
             if (fast) {
-                collide_two<C>(g, p.k, r_, u_, v_);
+                collide_two<C>(g, p.k, r_, u_, v_, mc);
             } else {
                 const uint2 cc = cring[((i - t + CR) & (CR - 1)) * 32 + lane];
                 // half-way bounce-back (and Ladd's moving-wall term) by selects
@@ -478,22 +505,27 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
                 if (win_inlet) {
                     const int R = yk - t;
                     const float lu = inlet_u(p.k, pyper ? wrap(R, p.H) : R);
-                    float f0[9], f1[9], rr[2], uu[2], vv[2];
+                    if constexpr (C::MLP) {
+                        collide_pair_mlp<Ph, true>(g, (cc.x & C_INLET) != 0, (cc.y & C_INLET) != 0, lu, p.k, mc.F,
+                                                   mc.stage, mc.zbuf, lane, r_, u_, v_);
+                    } else {
+                        float f0[9], f1[9], rr[2], uu[2], vv[2];
 #pragma unroll
-                    for (int q = 0; q < 9; ++q) {
-                        f0[q] = g[q].x;
-                        f1[q] = g[q].y;
+                        for (int q = 0; q < 9; ++q) {
+                            f0[q] = g[q].x;
+                            f1[q] = g[q].y;
+                        }
+                        collide_bf<Ph, true>(f0, (cc.x & C_INLET) != 0, lu, p.k, rr[0], uu[0], vv[0]);
+                        collide_bf<Ph, true>(f1, (cc.y & C_INLET) != 0, lu, p.k, rr[1], uu[1], vv[1]);
+#pragma unroll
+                        for (int q = 0; q < 9; ++q)
+                            g[q] = make_float2(f0[q], f1[q]);
+                        r_ = make_float2(rr[0], rr[1]);
+                        u_ = make_float2(uu[0], uu[1]);
+                        v_ = make_float2(vv[0], vv[1]);
                     }
-                    collide_bf<Ph, true>(f0, (cc.x & C_INLET) != 0, lu, p.k, rr[0], uu[0], vv[0]);
-                    collide_bf<Ph, true>(f1, (cc.y & C_INLET) != 0, lu, p.k, rr[1], uu[1], vv[1]);
-#pragma unroll
-                    for (int q = 0; q < 9; ++q)
-                        g[q] = make_float2(f0[q], f1[q]);
-                    r_ = make_float2(rr[0], rr[1]);
-                    u_ = make_float2(uu[0], uu[1]);
-                    v_ = make_float2(vv[0], vv[1]);
                 } else {
-                    collide_two<C>(g, p.k, r_, u_, v_);
+                    collide_two<C>(g, p.k, r_, u_, v_, mc);
                 }
                 if (C::MODE == MODE_CORE4) {
                     // cells that are not updated pass their values on (lbm_core4.cu's
@@ -615,14 +647,15 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
 // Launch constraints: TMA-aligned planes and mask (16-byte base, pitches and
 // plane strides multiples of 16 bytes), no periodic x (the TMA boxes do not
 // wrap), T in {2, 4, 6}.
-template <class E> inline bool rwave_ok(const WaveParams &p, int T, int mode)
+template <class E> inline bool rwave_ok(const WaveParams &p, int T, int mode, bool any_T = false)
 {
     const int es = (int)sizeof(E);
-    if (!(T == 2 || T == 4 || T == 6))
+    if (any_T ? !(T >= 1 && T <= 6) : !(T == 2 || T == 4 || T == 6))
         return false;
-    if (const char *e = getenv("LBM_KERNEL"))
-        if (e[0] == 'w') // LBM_KERNEL=wave: shared-memory wavefront kernel instead
-            return false;
+    if (!any_T)
+        if (const char *e = getenv("LBM_KERNEL"))
+            if (e[0] == 'w') // LBM_KERNEL=wave: shared-memory wavefront kernel instead
+                return false;
     if (mode == MODE_GENERAL && p.bc_left == LBM_BC_PERIODIC)
         return false;
     bool ok = aligned16(p.f_in) && aligned16(p.f_out) && ((long long)p.pitch * es) % 16 == 0 &&
@@ -685,7 +718,7 @@ template <class C> int launch_rwave(WaveParams p, cudaStream_t s)
         !make_map_mask(&tmm, p.mask, p.W, p.H, p.mask_pitch, C::BWM))
         return LBM_ERR_DEVICE;
     p.use_tma = 1;
-    const RwItems it = rw_items(p.W, p.H, C::CW, C::T, p.chunk);
+    const RwItems it = rw_items(p.W, p.H, C::CW, C::PADL, p.chunk);
     const int grid = (it.n_items + C::NW - 1) / C::NW;
     rwave_kernel<C><<<grid, 32 * C::NW, C::SMEM, s>>>(p, tmf, tmm);
     return status(cudaGetLastError());

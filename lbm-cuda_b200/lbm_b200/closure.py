@@ -1,0 +1,221 @@
+"""Learned closure: training data from filtered high-resolution runs of this
+solver, training on the GPU with the library's own forward / backward / Adam
+kernels (lbm_mlp_*), and packing for the collision kernel (LBM_CLOSURE_MLP).
+
+Model.  nu_t = out_scale * softplus(MLP(in_scale * x)), MLP 5 -> 32 -> 32 -> 1
+with SiLU; the collision relaxes the stress moments with 1 / (tau0 + 3 nu_t).
+The per-cell features x (what the kernel computes from the pre-collision
+populations) are the non-equilibrium stress moments n7 = Pi_xx - Pi_yy - rho
+(u^2 - v^2), n8 = Pi_xy - rho u v, the energy moment ne = e - rho (3 |u|^2 - 2),
+|(n7, n8)| and rho - 1.
+
+Training data (a priori).  A high-resolution run of decaying periodic
+turbulence (factor f finer, same flow in lattice units: nu_fine = f nu,
+f times as many steps) is box-filtered f x f onto the coarse grid.  At every
+snapshot the subgrid stress tau_ij = (u_i u_j)_bar - u_bar_i u_bar_j and the
+filtered strain S_ij (spectral derivatives) give the least-squares eddy
+viscosity nu* = max(0, -<tau^d : S> / (2 <S : S>)), <.> a 3 x 3 box average.
+The inputs follow the Chapman-Enskog forms of the same moments in the coarse
+solver: Pi^neq = -(2/3) tau_eff rho S with tau_eff = tau0 + 3 nu*, so
+n7 = -(2/3) tau_eff rho (S_xx - S_yy), n8 = -(2/3) tau_eff rho S_xy, and
+ne = -(2 / s_e) rho div(u).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import call, lib
+
+NI, NH = 5, 32
+NPARAM = NH * NI + NH + NH * NH + NH + NH + 1
+PACKED_BYTES = 4096
+OW1, OB1 = 0, NH * NI
+OW2 = OB1 + NH
+OB2 = OW2 + NH * NH
+OW3 = OB2 + NH
+OB3 = OW3 + NH
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """Xavier-uniform weights, zero biases (b3 so that softplus starts near 0.1)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(NPARAM, np.float32)
+
+    def xav(fan_in, fan_out, size):
+        a = np.sqrt(6.0 / (fan_in + fan_out))
+        return rng.uniform(-a, a, size).astype(np.float32)
+
+    p[OW1:OB1] = xav(NI, NH, NH * NI)
+    p[OW2:OB2] = xav(NH, NH, NH * NH)
+    p[OW3:OB3] = xav(NH, 1, NH)
+    p[OB3] = -2.25  # softplus(-2.25) ~ 0.1
+    return p
+
+
+class Mlp:
+    """The closure network with FP32 master parameters on the GPU."""
+
+    def __init__(self, params=None, in_scale=None, out_scale: float = 1.0, seed: int = 0):
+        import torch
+
+        p = init_params(seed) if params is None else np.asarray(params, np.float32)
+        self.params = torch.from_numpy(p.copy()).cuda()
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.step = 0
+        self.in_scale = np.ones(NI, np.float32) if in_scale is None else np.asarray(in_scale, np.float32)
+        self.out_scale = float(out_scale)
+        self._packed = None
+
+    def forward(self, x):
+        """softplus(MLP(x)) for x (n, 5) already scaled by in_scale (device tensors)."""
+        import torch
+
+        from . import _ptr, _stream
+
+        y = torch.empty(x.shape[0], dtype=torch.float32, device=x.device)
+        call("lbm_mlp_forward", _ptr(self.params), _ptr(x), _ptr(y), int(x.shape[0]), _stream(None))
+        return y
+
+    def loss_grad(self, x, t, w=None, workspace=None):
+        import torch
+
+        from . import _ptr, _stream
+
+        n = int(x.shape[0])
+        nbytes = int(lib().lbm_mlp_workspace_bytes(n))
+        if workspace is None or workspace.numel() * 4 < nbytes:
+            workspace = torch.empty((nbytes + 3) // 4, dtype=torch.float32, device=x.device)
+        grad = torch.empty(NPARAM, dtype=torch.float32, device=x.device)
+        loss = torch.empty(1, dtype=torch.float32, device=x.device)
+        call("lbm_mlp_grad", _ptr(self.params), _ptr(x), _ptr(t), _ptr(w), n, _ptr(grad), _ptr(loss),
+             _ptr(workspace), C.c_size_t(nbytes), _stream(None))
+        return loss, grad, workspace
+
+    def adam(self, grad, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
+        from . import _ptr, _stream
+
+        self.step += 1
+        call("lbm_mlp_adam", _ptr(self.params), _ptr(grad), _ptr(self.m), _ptr(self.v), self.step, float(lr),
+             float(beta1), float(beta2), float(eps), _stream(None))
+        self._packed = None
+
+    def fit(self, x_raw, nu, epochs: int = 200, batch: int = 16384, lr: float = 3e-3, seed: int = 0,
+            val_frac: float = 0.1):
+        """Trains on raw features (n, 5) and targets nu (n,) (numpy or torch);
+        sets in_scale / out_scale from the data.  Returns (train, validation) loss
+        histories (mean squared error in units of out_scale^2)."""
+        import torch
+
+        x_raw = torch.as_tensor(np.asarray(x_raw, np.float32)).cuda()
+        nu = torch.as_tensor(np.asarray(nu, np.float32)).cuda()
+        std = x_raw.std(dim=0).cpu().numpy()
+        self.in_scale = (1.0 / np.maximum(std, 1e-12)).astype(np.float32)
+        self.out_scale = float(max(nu.std().item(), 1e-12))
+        xs = x_raw * torch.from_numpy(self.in_scale).cuda()
+        ts = nu / self.out_scale
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        perm = torch.randperm(xs.shape[0], generator=g).cuda()
+        nval = max(1, int(val_frac * xs.shape[0]))
+        xv, tv = xs[perm[:nval]].contiguous(), ts[perm[:nval]].contiguous()
+        xt, tt = xs[perm[nval:]].contiguous(), ts[perm[nval:]].contiguous()
+        hist_t, hist_v = [], []
+        ws = None
+        n = xt.shape[0]
+        for ep in range(epochs):
+            order = torch.randperm(n, generator=g).cuda()
+            tot = 0.0
+            nb = 0
+            for b0 in range(0, n, batch):
+                idx = order[b0:b0 + batch]
+                loss, grad, ws = self.loss_grad(xt[idx].contiguous(), tt[idx].contiguous(), workspace=ws)
+                self.adam(grad, lr=lr * (0.5 * (1 + np.cos(np.pi * ep / epochs))))
+                tot += float(loss.item())
+                nb += 1
+            hist_t.append(tot / max(nb, 1))
+            lv, _, ws = self.loss_grad(xv, tv, workspace=ws)
+            hist_v.append(float(lv.item()))
+        return hist_t, hist_v
+
+    def predict(self, x_raw):
+        """nu_t for raw features (FP32 master weights)."""
+        import torch
+
+        xs = torch.as_tensor(np.asarray(x_raw, np.float32)).cuda() * torch.from_numpy(self.in_scale).cuda()
+        return self.forward(xs.contiguous()) * self.out_scale
+
+    def packed(self):
+        """Device buffer (LBM_MLP_PACKED_BYTES) for lbm_params.mlp."""
+        import torch
+
+        from . import _ptr, _stream
+
+        if self._packed is None:
+            buf = torch.zeros(PACKED_BYTES // 4, dtype=torch.float32, device="cuda")
+            sc = torch.from_numpy(self.in_scale).cuda()
+            call("lbm_mlp_pack", _ptr(self.params), _ptr(sc), float(self.out_scale), _ptr(buf), _stream(None))
+            self._packed = buf
+        return self._packed
+
+    def state(self) -> dict:
+        return {"params": self.params.cpu().numpy().tolist(), "in_scale": self.in_scale.tolist(),
+                "out_scale": self.out_scale}
+
+    @classmethod
+    def from_state(cls, st: dict) -> "Mlp":
+        return cls(params=np.array(st["params"], np.float32), in_scale=st["in_scale"], out_scale=st["out_scale"])
+
+
+# ---------------------------------------------------------------------------
+# training data from filtered high-resolution runs
+# ---------------------------------------------------------------------------
+def _deriv(a, axis):
+    N = a.shape[axis]
+    k = np.fft.fftfreq(N, d=1.0 / N) * 2.0 * np.pi / N
+    shape = [1, 1]
+    shape[axis] = N
+    return np.real(np.fft.ifft(1j * k.reshape(shape) * np.fft.fft(a, axis=axis), axis=axis))
+
+
+def strain(ux, uy):
+    """S_xx, S_yy, S_xy of a periodic field (spectral derivatives, lattice units)."""
+    dux_dx, dux_dy = _deriv(ux, 1), _deriv(ux, 0)
+    duy_dx, duy_dy = _deriv(uy, 1), _deriv(uy, 0)
+    return dux_dx, duy_dy, 0.5 * (dux_dy + duy_dx)
+
+
+def _box3(a):
+    return sum(np.roll(np.roll(a, i, 0), j, 1) for i in (-1, 0, 1) for j in (-1, 0, 1)) / 9.0
+
+
+def targets_and_features(u_f, v_f, rho_f, factor: int, tau0: float, s_e: float, nu_max: float = 0.05):
+    """Coarse features (n, 5) and least-squares eddy viscosities nu* (n,) from one
+    fine snapshot (fields (N f) x (N f))."""
+    from .spectral import box_filter
+
+    ub, vb, rb = box_filter(u_f, factor), box_filter(v_f, factor), box_filter(rho_f, factor)
+    tuu = box_filter(u_f * u_f, factor) - ub * ub
+    tvv = box_filter(v_f * v_f, factor) - vb * vb
+    tuv = box_filter(u_f * v_f, factor) - ub * vb
+    sxx, syy, sxy = strain(ub, vb)
+    tr = 0.5 * (tuu + tvv)
+    num = (tuu - tr) * sxx + (tvv - tr) * syy + 2.0 * tuv * sxy  # tau^d : S
+    den = sxx * sxx + syy * syy + 2.0 * sxy * sxy  # S : S
+    nu = np.clip(-_box3(num) / (2.0 * np.maximum(_box3(den), 1e-20)), 0.0, nu_max)
+    teff = tau0 + 3.0 * nu
+    n7 = -(2.0 / 3.0) * teff * rb * (sxx - syy)
+    n8 = -(2.0 / 3.0) * teff * rb * sxy
+    ne = -(2.0 / s_e) * rb * (sxx + syy)
+    x = np.stack([n7, n8, ne, np.hypot(n7, n8), rb - 1.0], axis=-1).reshape(-1, 5)
+    return x.astype(np.float32), nu.reshape(-1).astype(np.float32)
+
+
+def smagorinsky_nu(x, cs: float, tau0: float):
+    """The Smagorinsky eddy viscosity of the same features (the reference's
+    tau_eff = (tau0 + sqrt(tau0^2 + 18 Cs^2 Q / rho)) / 2, Q = |(n7, n8)|)."""
+    x = np.asarray(x, np.float64)
+    q, rho = x[:, 3], 1.0 + x[:, 4]
+    teff = 0.5 * (tau0 + np.sqrt(tau0 * tau0 + 18.0 * cs * cs * q / rho))
+    return (teff - tau0) / 3.0

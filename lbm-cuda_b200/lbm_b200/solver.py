@@ -8,7 +8,7 @@ from ._lib import call, lib
 
 STORE_F32, STORE_F16DEV, STORE_BF16DEV = 0, 1, 2
 COLL_BGK, COLL_MRT = 0, 1
-CLOSURE_NONE, CLOSURE_SMAG = 0, 1
+CLOSURE_NONE, CLOSURE_SMAG, CLOSURE_MLP = 0, 1, 2
 BC_WALL, BC_PERIODIC, BC_ZOUHE, BC_ZOUHE_RAMP, BC_OUTFLOW = 0, 1, 2, 3, 4
 
 
@@ -19,7 +19,7 @@ class Params(C.Structure):
         ("W", C.c_int), ("H", C.c_int), ("storage", C.c_int), ("collision", C.c_int), ("closure", C.c_int),
         ("s_nu", C.c_float), ("s_e", C.c_float), ("s_eps", C.c_float), ("s_q", C.c_float),
         ("cs_smag", C.c_float), ("bc_left", C.c_int), ("bc_right", C.c_int), ("bc_y", C.c_int),
-        ("u_in", C.c_float), ("u_lid", C.c_float), ("ref_clamps", C.c_int),
+        ("u_in", C.c_float), ("u_lid", C.c_float), ("ref_clamps", C.c_int), ("mlp", C.c_void_p),
     ]
 
 

@@ -492,11 +492,51 @@ void visualize(const float *ux, const float *uy, uint8_t *img, const uint8_t *ma
 //   * bc_right outflow: column W-1 is a ghost receiving the post-collision
 //     populations of x = W-2 (lbm_core4.cu:114-116);
 //   * cells that are not updated keep f_out's previous contents.
-// iparams = {W, H, collision(0 BGK, 1 MRT), closure(0 none, 1 Smagorinsky),
+// iparams = {W, H, collision(0 BGK, 1 MRT), closure(0 none, 1 Smagorinsky, 2 MLP),
 //            bc_left, bc_right, bc_y, ref_clamps}
 // dparams = {s_nu, s_e, s_eps, s_q, cs, u_in, u_lid}
 // BC codes: 0 wall, 1 periodic, 2 Zou-He, 3 Zou-He with ramp, 4 outflow.
 // ---------------------------------------------------------------------------
+// Learned closure (closure code 2): nu_t = out_scale softplus(MLP(in_scale x)),
+// MLP 5 -> 32 -> 32 -> 1 with SiLU, in double precision; x = (n7, n8, ne,
+// |(n7, n8)|, rho - 1) of the pre-collision populations.  Parameters: W1[32][5],
+// b1[32], W2[32][32], b2[32], w3[32], b3 (set by orc_set_mlp).
+struct MlpParams {
+    double p[32 * 5 + 32 + 32 * 32 + 32 + 32 + 1];
+    double in_scale[5];
+    double out_scale;
+    bool set;
+};
+static MlpParams g_mlp = {{0}, {0}, 1.0, false};
+
+template <class S> inline S mlp_rate(const S *f, S r, S u, S v, S tau0)
+{
+    const double n7 = double((f[1] - f[2] + f[3] - f[4]) - r * (u * u - v * v));
+    const double n8 = double((f[5] - f[6] + f[7] - f[8]) - r * u * v);
+    const double m1 = double(-S(4) * f[0] - (f[1] + f[2] + f[3] + f[4]) + S(2) * (f[5] + f[6] + f[7] + f[8]));
+    const double ne = m1 - double(r) * (3.0 * double(u * u + v * v) - 2.0);
+    const double x[5] = {n7, n8, ne, std::sqrt(n7 * n7 + n8 * n8), double(r) - 1.0};
+    const double *P = g_mlp.p;
+    double h1[32], h2[32];
+    for (int i = 0; i < 32; ++i) {
+        double a = P[160 + i];
+        for (int k = 0; k < 5; ++k)
+            a += P[i * 5 + k] * x[k] * g_mlp.in_scale[k];
+        h1[i] = a / (1.0 + std::exp(-a));
+    }
+    for (int i = 0; i < 32; ++i) {
+        double a = P[192 + 1024 + i];
+        for (int k = 0; k < 32; ++k)
+            a += P[192 + i * 32 + k] * h1[k];
+        h2[i] = a / (1.0 + std::exp(-a));
+    }
+    double z = P[192 + 1024 + 32 + 32];
+    for (int k = 0; k < 32; ++k)
+        z += P[192 + 1024 + 32 + k] * h2[k];
+    const double sp = z > 30.0 ? z : std::log1p(std::exp(z));
+    return S(1) / (tau0 + S(3.0 * g_mlp.out_scale * sp));
+}
+
 template <class S>
 void general_step(const int *ip, const double *dp, const uint8_t *mask, const S *fn, S *fo, S *ux, S *uy, S *rho)
 {
@@ -550,6 +590,8 @@ void general_step(const int *ip, const double *dp, const uint8_t *mask, const S 
                 }
                 if (clos == 1)
                     s = smag_rate(f, r, u, v, tau0, cs);
+                else if (clos == 2)
+                    s = mlp_rate(f, r, u, v, tau0);
             }
             ux[pid] = u;
             uy[pid] = v;
@@ -579,6 +621,16 @@ int orc_num_threads(void)
 #else
     return 1;
 #endif
+}
+
+void orc_set_mlp(const float *params, const float *in_scale, double out_scale)
+{
+    for (int i = 0; i < 32 * 5 + 32 + 32 * 32 + 32 + 32 + 1; ++i)
+        g_mlp.p[i] = params[i];
+    for (int k = 0; k < 5; ++k)
+        g_mlp.in_scale[k] = in_scale[k];
+    g_mlp.out_scale = out_scale;
+    g_mlp.set = true;
 }
 
 void orc_set_threads(int n)

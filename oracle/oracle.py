@@ -32,6 +32,7 @@ _SIGS = {
     "orc_general_step_f64": [_P] * 8,
     "orc_num_threads": [],
     "orc_set_threads": [_I],
+    "orc_set_mlp": [_P, _P, _D],
 }
 _RET = {"orc_num_threads": _I}
 
@@ -134,12 +135,19 @@ def visualize(ux, uy, mask, vort_scale=50.0, img=None):
 BC = {"wall": 0, "periodic": 1, "zouhe": 2, "zouhe_ramp": 3, "outflow": 4}
 
 
+def set_mlp(params, in_scale, out_scale):
+    """Weights of the oracle's learned closure (closure="mlp")."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    sc = np.ascontiguousarray(in_scale, dtype=np.float32)
+    lib().orc_set_mlp(_p(p), _p(sc), float(out_scale))
+
+
 class General:
     """Parameters of the general solver step (lbm_params semantics)."""
 
     def __init__(self, W, H, collision="mrt", closure="smag", s_nu=1.8, s_e=1.1, s_eps=1.1, s_q=1.1, cs=0.2,
                  bc_left="zouhe_ramp", bc_right="outflow", bc_y="wall", u_in=0.1, u_lid=0.0, ref_clamps=True):
-        self.ip = np.array([W, H, 1 if collision == "mrt" else 0, 1 if closure == "smag" else 0, BC[bc_left],
+        self.ip = np.array([W, H, 1 if collision == "mrt" else 0, {"none": 0, "smag": 1, "mlp": 2}[closure], BC[bc_left],
                             BC[bc_right], BC[bc_y], int(bool(ref_clamps))], dtype=np.int32)
         self.dp = np.array([s_nu, s_e, s_eps, s_q, cs, u_in, u_lid], dtype=np.float64)
 
