@@ -219,3 +219,140 @@ def smagorinsky_nu(x, cs: float, tau0: float):
     q, rho = x[:, 3], 1.0 + x[:, 4]
     teff = 0.5 * (tau0 + np.sqrt(tau0 * tau0 + 18.0 * cs * cs * q / rho))
     return (teff - tau0) / 3.0
+
+
+# ---------------------------------------------------------------------------
+# the decaying-turbulence judge and the a-posteriori comparison
+# ---------------------------------------------------------------------------
+def _run_periodic(N, f0, mask, n_steps, snap_every, T=2, **params):
+    """Periodic N x N run through the slab layer (one rank, so that the register
+    wavefront kernel applies); returns u, v, rho every snap_every steps (incl. 0)."""
+    import torch
+
+    from . import solver as SV
+    from .slab import SlabSolver
+
+    # halo >= T with N + 2 halo a multiple of 16 (TMA row pitch of the mask)
+    halo = T
+    while (N + 2 * halo) % 16:
+        halo += 1
+    S = SlabSolver(N, N, mask, T=T, halo=halo, bc_left=SV.BC_PERIODIC, bc_right=SV.BC_PERIODIC,
+                   bc_y=SV.BC_PERIODIC, **params)
+    S.set_state(torch.as_tensor(f0))
+    snaps = []
+
+    def macros():
+        f = S.gather().double()
+        if S.storage != SV.STORE_F32:
+            w = torch.tensor([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, dtype=torch.float64, device=f.device)
+            f = f + w[:, None, None]
+        cx = torch.tensor([0, 1, 0, -1, 0, 1, -1, -1, 1], dtype=torch.float64, device=f.device)[:, None, None]
+        cy = torch.tensor([0, 0, 1, 0, -1, 1, 1, -1, -1], dtype=torch.float64, device=f.device)[:, None, None]
+        r = f.sum(0)
+        return ((f * cx).sum(0) / r).cpu().numpy(), ((f * cy).sum(0) / r).cpu().numpy(), r.cpu().numpy()
+
+    snaps.append(macros())
+    done = 0
+    while done < n_steps:
+        k = min(snap_every, n_steps - done)
+        S.run(k)
+        done += k
+        snaps.append(macros())
+    return snaps
+
+
+def filtered_judge(N: int, factor: int = 4, k0: float = 4.0, u_rms: float = 0.1 * 0.5773502691896258,
+                   nu: float = 5e-4, n_steps: int = 600, snap_every: int = 100, seed: int = 0, fine_cs: float = 0.0):
+    """Runs the factor-finer decaying turbulence (MRT, nu_fine = factor nu,
+    factor n_steps steps) and returns its snapshots filtered onto N x N, the
+    coarse initial state, and a-priori training data (features, nu*) per snapshot."""
+    import torch
+
+    from . import solver as SV
+    from .init import equilibrium
+    from .spectral import box_filter, random_phase_velocity
+
+    Nf = N * factor
+    ux, uy = random_phase_velocity(Nf, k0, u_rms, seed)
+    f0 = equilibrium(np.ones((Nf, Nf)), ux, uy, dtype=np.float32)
+    nu_f = factor * nu
+    tau_f = 3.0 * nu_f + 0.5
+    mask = torch.zeros((Nf, Nf), dtype=torch.uint8)
+    closure = dict(closure=SV.CLOSURE_SMAG, cs_smag=fine_cs) if fine_cs > 0 else dict(closure=SV.CLOSURE_NONE)
+    snaps = _run_periodic(Nf, f0, mask, factor * n_steps, factor * snap_every, s_nu=1.0 / tau_f, ref_clamps=0,
+                          **closure)
+    tau0 = 3.0 * nu + 0.5
+    judge, data = [], []
+    for (u, v, r) in snaps:
+        judge.append((box_filter(u, factor), box_filter(v, factor)))
+        if not (np.isfinite(u).all() and np.isfinite(v).all()):
+            raise FloatingPointError("the high-resolution run became unstable; raise its viscosity or Smagorinsky "
+                                     "constant")
+        data.append(targets_and_features(u, v, r, factor, tau0=tau0, s_e=1.1))
+    ub, vb = box_filter(ux, factor), box_filter(uy, factor)
+    fc = equilibrium(np.ones((N, N)), ub, vb, dtype=np.float32)
+    return {"judge": judge, "data": data, "coarse_f0": fc, "tau0": tau0, "N": N, "factor": factor,
+            "snap_every": snap_every, "n_steps": n_steps}
+
+
+def velocity_error(snaps, judge):
+    """Relative L2 velocity error of each snapshot against the judge."""
+    out = []
+    for (u, v, _), (uj, vj) in zip(snaps, judge):
+        num = np.sqrt(np.sum((u - uj) ** 2 + (v - vj) ** 2))
+        den = np.sqrt(np.sum(uj ** 2 + vj ** 2))
+        out.append(float(num / den))
+    return out
+
+
+def spectrum_error(snaps, judge):
+    """L2 distance of log10 energy spectra (shells 1 .. N/2) to the judge's, per snapshot."""
+    from .spectral import energy_spectrum
+
+    out = []
+    for (u, v, _), (uj, vj) in zip(snaps, judge):
+        _, e = energy_spectrum(u, v)
+        _, ej = energy_spectrum(uj, vj)
+        a, b = np.log10(np.maximum(e[1:], 1e-30)), np.log10(np.maximum(ej[1:], 1e-30))
+        out.append(float(np.sqrt(np.mean((a - b) ** 2))))
+    return out
+
+
+def compare_closures(J, net: "Mlp", cs: float = 0.1, storage: int = 0, T: int = 2):
+    """Coarse runs from the filtered initial state with no closure, Smagorinsky
+    (Cs) and the network; relative L2 velocity error and log-spectrum error
+    against the judge per snapshot, for each: {name: (l2, spectrum)}."""
+    import torch
+
+    from . import solver as SV
+
+    N = J["N"]
+    mask = torch.zeros((N, N), dtype=torch.uint8)
+    base = dict(s_nu=1.0 / J["tau0"], ref_clamps=0, storage=storage)
+    res = {}
+    for name, extra in (("none", dict(closure=SV.CLOSURE_NONE)), ("smagorinsky", dict(closure=SV.CLOSURE_SMAG,
+                                                                                           cs_smag=cs)),
+                        ("mlp", dict(closure=SV.CLOSURE_MLP, mlp=net.packed().data_ptr()))):
+        f0 = J["coarse_f0"]
+        if storage != SV.STORE_F32:
+            f0 = f0 - np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, np.float32)[:, None, None]
+            f0 = torch.from_numpy(f0).to(torch.float16 if storage == SV.STORE_F16DEV else torch.bfloat16)
+        snaps = _run_periodic(N, f0, mask, J["n_steps"], J["snap_every"], T=T, **base, **extra)
+        res[name] = (velocity_error(snaps, J["judge"]), spectrum_error(snaps, J["judge"]))
+    return res
+
+
+def a_priori(J, train_snaps, test_snaps, epochs: int = 120, seed: int = 0, cs: float = 0.1):
+    """Trains a network on the a-priori data of train_snaps and returns it with
+    the mean squared eddy-viscosity error on test_snaps of the network, of
+    Smagorinsky (Cs) and of no closure (nu_t = 0)."""
+    x = np.concatenate([J["data"][i][0] for i in train_snaps])
+    y = np.concatenate([J["data"][i][1] for i in train_snaps])
+    xt = np.concatenate([J["data"][i][0] for i in test_snaps])
+    yt = np.concatenate([J["data"][i][1] for i in test_snaps])
+    net = Mlp(seed=seed)
+    net.fit(x, y, epochs=epochs, batch=8192, lr=3e-3, seed=seed)
+    pm = net.predict(xt).cpu().numpy()
+    ps = smagorinsky_nu(xt, cs, J["tau0"])
+    return net, {"mlp": float(np.mean((pm - yt) ** 2)), "smagorinsky": float(np.mean((ps - yt) ** 2)),
+                 "none": float(np.mean(yt ** 2))}
