@@ -182,6 +182,9 @@ def main():
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32",
                     help="population storage of the cylinder workload (16-bit: deviations f - w)")
     ap.add_argument("--workload", choices=["cylinder", "batch", "dropins"], default="cylinder")
+    ap.add_argument("--closure", choices=["smag", "mlp"], default="smag",
+                    help="mlp: the learned closure (random-initialised weights of the 5-32-32-1 network, "
+                         "no reference clamps) in place of Smagorinsky")
     args = ap.parse_args()
 
     rank, world, local = dist_env()
@@ -236,7 +239,13 @@ def main():
     b_alg = B_ALG if storage == SV.STORE_F32 else B_ALG / 2
     mask_np, f0_np = workload()
     mask = torch.from_numpy(mask_np).cuda()
-    S = Solver(W, H, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU, storage=storage)
+    extra = {}
+    if args.closure == "mlp":
+        from lbm_b200.closure import Mlp
+
+        net = Mlp(seed=0, in_scale=np.array([1e3, 1e3, 1e3, 1e3, 1e2], np.float32), out_scale=1e-4)
+        extra = dict(closure=SV.CLOSURE_MLP, mlp=net.packed().data_ptr(), ref_clamps=0)
+    S = Solver(W, H, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU, storage=storage, **extra)
     f_a = torch.empty((9, H, W), dtype=S.dtype, device="cuda")
     SV.convert_state(torch.from_numpy(f0_np).cuda(), SV.STORE_F32, f_a, storage)
     f_b = f_a.clone()
@@ -313,6 +322,8 @@ def main():
         achieved = b_alg * W * H * T / (launch_ms * 1e-3) / 1e9
         traffic = None
         kname = "stream_kernel" if T == 1 else ("rwave_kernel" if T in (2, 4, 6) else "wave_kernel")
+        if args.closure == "mlp":
+            kname = "rwave_kernel_mlp"
         suffix = "" if args.storage == "f32" else "_" + args.storage
         tfile = os.path.join(ROOT, "profiles", f"{kname}_T{T}_{W}x{H}{suffix}_traffic.json")
         if os.path.exists(tfile):
@@ -335,7 +346,7 @@ def main():
             "data": "synthetic",
             "config": {"workload": f"cylinder channel {W}x{H} D2Q9 MRT+Smagorinsky Cs={CS}, Zou-He u={U_IN}, "
                                    f"D={CYL[2]} at ({CYL[0]},{CYL[1]}), nu={NU}, T={T} steps per launch",
-                       "storage": args.storage,
+                       "storage": args.storage, "closure": args.closure,
                        "W": W, "H": H, "T": T, "physical_steps_per_step": n_launch * T,
                        "l2": "inputs larger than L2 (two 151 MB population buffers)",
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},

@@ -6,15 +6,17 @@
 //   w1[32][16]  first layer, feature k (k < 5) pre-multiplied by in_scale[k],
 //               column 5 holds b1 (the staged features carry a constant 1
 //               there), columns 6..15 zero;
-//   w2[32][32], w3[8][32] (row 0 = w3, rows 1..7 zero), b2[32], b3, out_scale.
+//   w2[32][32], w3[8][32] (row 0 = w3, rows 1..7 zero), b2[32], b3, out_scale;
+//   w1, b1, w2 and b2 are stored at half scale (see silu_half_bf16x2).
 //
 // Per warp: the 64 feature rows are staged as BF16 in 1 KB of shared memory
 // (row c = cell c = 2 lane + n, 8 values: 5 features, 1, 0, 0) and read as A
 // fragments; a layer's accumulators become the next layer's A fragments in
 // registers (the m16n8k16 accumulator layout of two adjacent 8-column tiles is
 // the A layout of one 16-wide k tile).  SiLU runs on BF16 pairs:
-// silu(h) = h/2 (1 + tanh(h/2)) with tanh.approx.bf16x2, one transcendental per
-// two activations.  The output z of a cell is nu_t = out_scale softplus(z).
+// silu(a) = a/2 (1 + tanh(a/2)) with tanh.approx.bf16x2, one transcendental per
+// two activations (on the half-scale accumulators).  The output z of a cell is
+// nu_t = out_scale softplus(z).
 #pragma once
 
 #include "collide.cuh"
@@ -86,13 +88,13 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
     return d;
 }
 
-// silu of a BF16 pair: h/2 (1 + tanh(h/2)).
-__device__ __forceinline__ uint32_t silu_bf16x2(uint32_t h)
+// silu(a) of a BF16 pair given h = a/2 (the packed layers are at half scale):
+// a sigmoid(a) = a/2 (1 + tanh(a/2)) = h + h tanh(h).
+__device__ __forceinline__ uint32_t silu_half_bf16x2(uint32_t h)
 {
-    uint32_t hh, th, r;
-    asm("mul.rn.bf16x2 %0, %1, %2;" : "=r"(hh) : "r"(h), "r"(0x3F003F00u));
-    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(hh));
-    asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(r) : "r"(hh), "r"(th), "r"(hh));
+    uint32_t th, r;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(h));
+    asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(r) : "r"(h), "r"(th), "r"(h));
     return r;
 }
 
@@ -133,10 +135,10 @@ __device__ __forceinline__ void mlp_nu_t(const MlpFrag &F, const float (&x)[2][5
         uint32_t a2[2][4];
 #pragma unroll
         for (int kt = 0; kt < 2; ++kt) {
-            a2[kt][0] = silu_bf16x2(pack_bf16x2(h1[2 * kt][0], h1[2 * kt][1]));
-            a2[kt][1] = silu_bf16x2(pack_bf16x2(h1[2 * kt][2], h1[2 * kt][3]));
-            a2[kt][2] = silu_bf16x2(pack_bf16x2(h1[2 * kt + 1][0], h1[2 * kt + 1][1]));
-            a2[kt][3] = silu_bf16x2(pack_bf16x2(h1[2 * kt + 1][2], h1[2 * kt + 1][3]));
+            a2[kt][0] = silu_half_bf16x2(pack_bf16x2(h1[2 * kt][0], h1[2 * kt][1]));
+            a2[kt][1] = silu_half_bf16x2(pack_bf16x2(h1[2 * kt][2], h1[2 * kt][3]));
+            a2[kt][2] = silu_half_bf16x2(pack_bf16x2(h1[2 * kt + 1][0], h1[2 * kt + 1][1]));
+            a2[kt][3] = silu_half_bf16x2(pack_bf16x2(h1[2 * kt + 1][2], h1[2 * kt + 1][3]));
         }
         float h2[4][4];
 #pragma unroll
@@ -152,10 +154,10 @@ __device__ __forceinline__ void mlp_nu_t(const MlpFrag &F, const float (&x)[2][5
         uint32_t a3[2][4];
 #pragma unroll
         for (int kt = 0; kt < 2; ++kt) {
-            a3[kt][0] = silu_bf16x2(pack_bf16x2(h2[2 * kt][0], h2[2 * kt][1]));
-            a3[kt][1] = silu_bf16x2(pack_bf16x2(h2[2 * kt][2], h2[2 * kt][3]));
-            a3[kt][2] = silu_bf16x2(pack_bf16x2(h2[2 * kt + 1][0], h2[2 * kt + 1][1]));
-            a3[kt][3] = silu_bf16x2(pack_bf16x2(h2[2 * kt + 1][2], h2[2 * kt + 1][3]));
+            a3[kt][0] = silu_half_bf16x2(pack_bf16x2(h2[2 * kt][0], h2[2 * kt][1]));
+            a3[kt][1] = silu_half_bf16x2(pack_bf16x2(h2[2 * kt][2], h2[2 * kt][3]));
+            a3[kt][2] = silu_half_bf16x2(pack_bf16x2(h2[2 * kt + 1][0], h2[2 * kt + 1][1]));
+            a3[kt][3] = silu_half_bf16x2(pack_bf16x2(h2[2 * kt + 1][2], h2[2 * kt + 1][3]));
         }
         float z[4] = {F.b3v, 0.0f, F.b3v, 0.0f};
 #pragma unroll

@@ -218,6 +218,9 @@ __global__ void mlp_adam_kernel(float *params, const float *grad, float *m, floa
     params[p] -= lr * (mm * c1) / (sqrtf(vv * c2) + eps);
 }
 
+// The hidden layers are stored at half scale (W1, b1, W2, b2 times 1/2): the
+// kernel's accumulators then hold a/2, and silu(a) = a/2 (1 + tanh(a/2)) is one
+// tanh and one fma on them.
 __global__ void mlp_pack_kernel(const float *P, const float *in_scale, float out_scale, MlpPacked *W)
 {
     const int tid = threadIdx.x;
@@ -228,14 +231,14 @@ __global__ void mlp_pack_kernel(const float *P, const float *in_scale, float out
             v = P[OW1 + n * NI + k] * in_scale[k];
         else if (k == NI)
             v = P[OB1 + n];
-        W->w1[n][k] = __float2bfloat16_rn(v);
+        W->w1[n][k] = __float2bfloat16_rn(0.5f * v);
     }
     for (int i = tid; i < 32 * 32; i += blockDim.x)
-        W->w2[i / 32][i % 32] = __float2bfloat16_rn(P[OW2 + i]);
+        W->w2[i / 32][i % 32] = __float2bfloat16_rn(0.5f * P[OW2 + i]);
     for (int i = tid; i < 8 * 32; i += blockDim.x)
         W->w3[i / 32][i % 32] = __float2bfloat16_rn(i < 32 ? P[OW3 + i] : 0.0f);
     for (int i = tid; i < 32; i += blockDim.x)
-        W->b2[i] = P[OB2 + i];
+        W->b2[i] = 0.5f * P[OB2 + i];
     if (tid == 0) {
         W->b3 = P[OB3];
         W->out_scale = out_scale;
