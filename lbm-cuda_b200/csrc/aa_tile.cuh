@@ -36,7 +36,31 @@ struct AaParams {
     int use_tma;
     int *err;
     Phys k;
+    // Edge-only launch (1-D grid): skip the tiles with etx0 <= tx < etx1 and
+    // ety0 <= ty < ety1 (computed by another kernel); nx tile columns.
+    int edge_only, etx0, etx1, ety0, ety1, nx;
 };
+
+// Tile coordinates of 1-D block b of an edge-only launch: the tile rows below
+// ety0 in full, then the rows [ety0, ety1) with only their edge columns, then
+// the rows from ety1 on in full.
+__device__ __forceinline__ void aa_edge_tile(const AaParams &p, int b, int &tx, int &ty)
+{
+    const int top = p.ety0 * p.nx;
+    const int nl = p.etx0, nr = p.nx - p.etx1, mid = (p.ety1 - p.ety0) * (nl + nr);
+    if (b < top) {
+        tx = b % p.nx;
+        ty = b / p.nx;
+    } else if (b < top + mid) {
+        const int j = b - top, r = j / (nl + nr), c = j % (nl + nr);
+        ty = p.ety0 + r;
+        tx = c < nl ? c : p.etx1 + (c - nl);
+    } else {
+        const int j = b - top - mid;
+        tx = j % p.nx;
+        ty = p.ety1 + j / p.nx;
+    }
+}
 
 template <int T_, int VAR_, int SX_ = 64, int SY_ = 32, int NT_ = 256, int NB_ = 4, int MINB_ = 2> struct AaCfg {
     static constexpr int T = T_;
@@ -85,8 +109,11 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
     const int col = (tid & 31) + 32 * ((tid >> 5) % C::WPR); // 0..SX-1
     const int rb = (tid >> 5) / C::WPR;                       // 0..RSTEP-1
     constexpr int RS = C::RSTEP;
-    const int xt = blockIdx.x * CX - T;                // global x of tile column 0
-    const int yt = blockIdx.y * CY - T;
+    int tile_x = blockIdx.x, tile_y = blockIdx.y;
+    if (p.edge_only)
+        aa_edge_tile(p, blockIdx.x, tile_x, tile_y);
+    const int xt = tile_x * CX - T; // global x of tile column 0
+    const int yt = tile_y * CY - T;
     const bool tma = p.use_tma != 0;
     const int xf = tma ? floor_div(xt, 4) * 4 : xt; // global x of smem row entry 0
     const int xm = tma ? floor_div(xt, 16) * 16 : xt;

@@ -4,8 +4,11 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "aa_tile.cuh"
 #include "host.h"
+#include "rwave.cuh"
 
 namespace lbm {
 
@@ -37,6 +40,34 @@ template <class C> int launch_aa(AaParams p, cudaStream_t s)
     return status(cudaGetLastError());
 }
 
+// The tile kernel on an explicit 1-D grid (edge-only launches).
+template <class C> int launch_aa_grid(AaParams p, int nblocks, cudaStream_t s)
+{
+    static int attr_done[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr_done[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(aa_tile_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        if (e != cudaSuccess)
+            return status(e);
+        attr_done[dev] = 1;
+    }
+    if (!p.err)
+        p.err = device_error_word();
+    CUtensorMap tmf, tmm;
+    memset(&tmf, 0, sizeof(tmf));
+    memset(&tmm, 0, sizeof(tmm));
+    bool tma = p.use_tma && aligned16(p.f_in) && aligned16(p.mask) && (p.W % 16) == 0;
+    if (tma)
+        tma = make_map_planes(&tmf, p.f_in, 4, p.W, p.H, p.W, (long long)p.W * p.H, C::SW, C::SY) &&
+              make_map_mask(&tmm, p.mask, p.W, p.H, p.W, C::MW, C::SY);
+    p.use_tma = tma ? 1 : 0;
+    aa_tile_kernel<C><<<nblocks, C::NT, C::SMEM, s>>>(p, tmf, tmm);
+    return status(cudaGetLastError());
+}
+
+template <class Cfg, int MODE> static int aa_split(AaParams p, int T, cudaStream_t s, bool &done);
+
 // Tile shapes: (SX, SY, threads, cells per batch, CTAs per SM).  Shape 0 is a
 // 64 x 32 tile (less halo recomputation), shape 1 a 32 x 32 tile with more
 // CTAs per SM (more warps to hide latency).
@@ -44,6 +75,17 @@ template <int VAR, int SHAPE> static int aa_dispatch_shape(const AaParams &p, in
 {
     constexpr int SX = SHAPE == 0 ? 64 : 32, SY = 32, NT = SHAPE == 0 ? 256 : 256, NB = SHAPE == 0 ? 4 : 2;
     constexpr int MB = SHAPE == 0 ? 2 : 3;
+    constexpr int MODE = VAR == VARIANT_SMEMAA ? MODE_PRE_SMEMAA : MODE_PRE_POLICY;
+    bool done = false;
+    int rc = LBM_OK;
+    if (T == 2)
+        rc = aa_split<AaCfg<2, VAR, SX, SY, NT, NB, MB>, MODE>(p, T, s, done);
+    else if (T == 4)
+        rc = aa_split<AaCfg<4, VAR, SX, SY, NT, NB, MB>, MODE>(p, T, s, done);
+    else if (T == 6)
+        rc = aa_split<AaCfg<6, VAR, SX, SY, NT, NB, MB>, MODE>(p, T, s, done);
+    if (rc || done)
+        return rc;
     switch (T) {
     case 2:
         return launch_aa<AaCfg<2, VAR, SX, SY, NT, NB, MB>>(p, s);
@@ -66,6 +108,121 @@ template <int VAR> static int aa_dispatch(const AaParams &p, int T, cudaStream_t
         shape = (e && atoi(e) == 0) ? 0 : 1;
     }
     return shape == 0 ? aa_dispatch_shape<VAR, 0>(p, T, s) : aa_dispatch_shape<VAR, 1>(p, T, s);
+}
+
+// Split launch for T = 2, 4, 6 on TMA-aligned buffers: the reference's AA slot
+// semantics differ from plain collide-then-stream only near x = 0 (Zou-He and the
+// stale inlet slots), x = W-2 / W-1 (stale outlet slots, the ghost copy) and the
+// first and last rows; the shared-memory AA tile kernel runs on the tiles of that
+// edge band, and the register wavefront kernel in pre-collision mode on the
+// interior rectangle (tile-aligned, at least T + 2 cells from every edge), where
+// both give the same values.  LBM_AA_SPLIT=0 runs the tile kernel everywhere.
+// Side stream and events per device for running the edge-band kernel beside the
+// interior kernel (fork on an event of the caller's stream, join on another);
+// event waits keep the pair capturable into a CUDA graph.
+struct SplitStreams {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+static int split_streams(SplitStreams **out)
+{
+    static SplitStreams per_dev[64];
+    static std::mutex mu;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess)
+        return status(e);
+    if (dev < 0 || dev >= 64)
+        return LBM_ERR_DEVICE;
+    std::lock_guard<std::mutex> lock(mu);
+    SplitStreams &ss = per_dev[dev];
+    if (!ss.side) {
+        if ((e = cudaStreamCreateWithFlags(&ss.side, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming)) != cudaSuccess)
+            return status(e);
+    }
+    *out = &ss;
+    return LBM_OK;
+}
+
+template <class Cfg, int MODE>
+static int aa_split(AaParams p, int T, cudaStream_t s, bool &done)
+{
+    done = false;
+    if (const char *e = getenv("LBM_AA_SPLIT"))
+        if (atoi(e) == 0)
+            return LBM_OK;
+    constexpr int CX = Cfg::CX, CY = Cfg::CY;
+    const int W = p.W, H = p.H;
+    const bool al = aligned16(p.f_in) && aligned16(p.f_out) && aligned16(p.mask) && W % 16 == 0 &&
+                    (!p.ux || (aligned16(p.ux) && aligned16(p.uy) && aligned16(p.rho)));
+    const int nx = (W + CX - 1) / CX, ny = (H + CY - 1) / CY;
+    const int etx0 = (T + 2 + CX - 1) / CX, etx1 = (W - T - 3) / CX;
+    const int ety0 = (T + 2 + CY - 1) / CY, ety1 = (H - T - 2) / CY;
+    // the split pays on domains larger than the L2 cache (measured: 1.3x the tile
+    // kernel at 4096 x 1024, 0.8x at 2048 x 512 where the interior is too small to
+    // fill the GPU with full-length work items)
+    if (!al || etx1 - etx0 < 2 || ety1 - ety0 < 1 || (CX & 1) || (long long)W * H < (4ll << 20))
+        return LBM_OK;
+    // edge band: the tile kernel on the tiles outside the interior block
+    p.edge_only = 1;
+    p.etx0 = etx0;
+    p.etx1 = etx1;
+    p.ety0 = ety0;
+    p.ety1 = ety1;
+    p.nx = nx;
+    const int nedge = nx * ny - (etx1 - etx0) * (ety1 - ety0);
+    SplitStreams *ss = nullptr;
+    int rc = split_streams(&ss);
+    if (rc)
+        return rc;
+    cudaError_t e;
+    if ((e = cudaEventRecord(ss->fork, s)) != cudaSuccess || (e = cudaStreamWaitEvent(ss->side, ss->fork, 0)) != cudaSuccess)
+        return status(e);
+    rc = launch_aa_grid<Cfg>(p, nedge, ss->side);
+    if (rc)
+        return rc;
+    if ((e = cudaEventRecord(ss->join, ss->side)) != cudaSuccess)
+        return status(e);
+    // interior: pre-collision register wavefront
+    WaveParams w;
+    memset(&w, 0, sizeof(w));
+    w.f_in = p.f_in;
+    w.f_out = p.f_out;
+    w.mask = p.mask;
+    w.ux = p.ux;
+    w.uy = p.uy;
+    w.rho = p.rho;
+    w.W = W;
+    w.H = H;
+    w.pitch = W;
+    w.plane = (long long)W * H;
+    w.mask_pitch = W;
+    w.bc_left = w.bc_right = w.bc_y = LBM_BC_WALL;
+    w.use_tma = 1;
+    w.k = p.k;
+    w.rx0 = etx0 * CX;
+    w.rx1 = etx1 * CX;
+    w.ry0 = ety0 * CY;
+    w.ry1 = ety1 * CY;
+    switch (T) {
+    case 2:
+        rc = launch_rwave<RwCfg<2, 1, 1, PhysBgkRef, StoreF32, MODE>>(w, s);
+        break;
+    case 4:
+        rc = launch_rwave<RwCfg<4, 1, 2, PhysBgkRef, StoreF32, MODE>>(w, s);
+        break;
+    case 6:
+        rc = launch_rwave<RwCfg<6, 1, 2, PhysBgkRef, StoreF32, MODE>>(w, s);
+        break;
+    default:
+        rc = LBM_ERR_UNSUPPORTED;
+    }
+    // join: the caller's stream continues after both kernels
+    e = cudaStreamWaitEvent(s, ss->join, 0);
+    done = true;
+    return rc ? rc : status(e);
 }
 
 static AaParams aa_params(const uint8_t *mask, const float *f_now, float *f_out, float *ux, float *uy, float *rho,

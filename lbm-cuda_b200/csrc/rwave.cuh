@@ -274,6 +274,22 @@ __host__ __device__ __forceinline__ void rw_item(const RwItems &it, int item, in
     }
 }
 
+// rho, u, v of a lane's two cells in the reference's summation order.
+__device__ __forceinline__ void moments_pair(const float2 (&g)[9], float2 &r, float2 &u, float2 &v)
+{
+    float f0[9], f1[9], r0, u0, v0, r1, u1, v1;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        f0[q] = g[q].x;
+        f1[q] = g[q].y;
+    }
+    moments_seq(f0, r0, u0, v0);
+    moments_seq(f1, r1, u1, v1);
+    r = make_float2(r0, r1);
+    u = make_float2(u0, u1);
+    v = make_float2(v0, v1);
+}
+
 // Per-warp state of the learned closure (unused by the other variants).
 struct MlpCtx {
     MlpFrag F;
@@ -330,12 +346,18 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wi = threadIdx.x >> 5;
-    const RwItems items = rw_items(p.W, p.H, C::CW, C::PADL, p.chunk);
+    constexpr bool PRE = C::MODE == MODE_PRE_SMEMAA || C::MODE == MODE_PRE_POLICY;
+    // output rectangle [rx0, rx1) x [ry0, ry1) (the whole domain unless set)
+    const int rx0 = p.rx1 > 0 ? p.rx0 : 0, rx1 = p.rx1 > 0 ? p.rx1 : p.W;
+    const int ry0 = p.ry1 > 0 ? p.ry0 : 0, ry1 = p.ry1 > 0 ? p.ry1 : p.H;
+    const RwItems items = rw_items(rx1 - rx0, ry1 - ry0, C::CW, C::PADL, p.chunk);
     const int item = blockIdx.x * C::NW + wi;
     if (item >= items.n_items)
         return; // whole warp: no item left (nothing below waits on other warps)
     int win, ya, yb;
-    rw_item(items, item, p.H, p.chunk, win, ya, yb);
+    rw_item(items, item, ry1 - ry0, p.chunk, win, ya, yb);
+    ya += ry0;
+    yb += ry0;
 
     unsigned char *wbase = smem + wi * C::WARP_BYTES;
     uint64_t *bar = reinterpret_cast<uint64_t *>(wbase);
@@ -350,7 +372,7 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
         mlp_load_frag(static_cast<const MlpPacked *>(p.k.mlp), mc.F, lane);
     }
 
-    const int xs = win * C::CW - C::PADL;
+    const int xs = rx0 + win * C::CW - C::PADL;
     const int x = xs + 2 * lane; // column of the lane's first cell
     const int row0 = ya - T;
     const int nrows = yb - ya + 2 * T;
@@ -360,7 +382,7 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
     const int offf = (xs - xa) + 2 * lane; // element offset of the lane's pair in a ring row
     const int offm = (xs - xm) + 2 * lane; // byte offset of the lane's mask pair
     // Columns at or next to the domain's left/right ends are always special.
-    const bool colspec = x <= 0 || x + 1 >= p.W - 2;
+    const bool colspec = !PRE && (x <= 0 || x + 1 >= p.W - 2);
     const bool core0 = 2 * lane >= C::PADL && 2 * lane < 64 - C::PADL;
     // Window-wide work of the generic body: Zou-He inlet and outlet ghost.
     const bool win_inlet =
@@ -432,6 +454,29 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
         const E *rN = reinterpret_cast<const E *>(ring + s0 * C::SLOT) + offf;
         const E *rO = reinterpret_cast<const E *>(ring + s1 * C::SLOT) + offf;
         const E *rS = reinterpret_cast<const E *>(ring + s2 * C::SLOT) + offf;
+        if constexpr (PRE) {
+            // collide the new row in place (its own cells only): the ring then holds
+            // post-collision values, which the levels above stream and collide
+            float *rw = reinterpret_cast<float *>(ring + s0 * C::SLOT) + offf;
+            const uint32_t om =
+                *reinterpret_cast<const uint16_t *>(ring + s0 * C::SLOT + C::SLOT_F + offm); // own mask bytes
+            float2 g[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                g[q] = ld2(rw + q * BW, q);
+            float2 rr, uu, vv;
+            float2 c[9];
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                c[q] = g[q];
+            collide_two<C>(c, p.k, rr, uu, vv, mc);
+            const bool sk0 = (om & 0xffu) != 0u, sk1 = (om >> 8) != 0u;
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+                st2(rw + q * BW, make_float2(sk0 ? g[q].x : c[q].x, sk1 ? g[q].y : c[q].y), q);
+            fence_proxy_async(); // these generic writes precede the slot's next TMA refill
+            __syncwarp();
+        }
 
         // ---- codes of level 1's row (yk - 1) from mask rows yk-2 .. yk ----
         {
@@ -446,14 +491,17 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
                 mw[d] = ((lft >> 8) & 0xffu) | (own << 8) | ((rgt & 0xffu) << 24);
             }
             const int R1 = yk - 1;
-            const bool rowspec = !pyper && (R1 <= 0 || R1 >= p.H - 1);
+            const bool rowspec = !PRE && !pyper && (R1 <= 0 || R1 >= p.H - 1);
             const bool spec = colspec || rowspec || ((mw[0] | mw[1] | mw[2]) != 0u);
             const bool wspec = __any_sync(M, spec);
             hist = (hist << 1) | (wspec ? 1u : 0u);
             uint2 cc = make_uint2(0u, 0u);
             if (wspec) {
                 uint32_t c2[2];
-                codes_from_bytes<C::MODE, C::LID>(mw, oob_cols, x, R1, p.W, p.H, p.bc_left, p.bc_right, pyper, c2);
+                codes_from_bytes<PRE ? (int)MODE_GENERAL : C::MODE, C::LID>(mw, oob_cols, x, R1, p.W, p.H,
+                                                                            PRE ? (int)LBM_BC_WALL : p.bc_left,
+                                                                            PRE ? (int)LBM_BC_WALL : p.bc_right,
+                                                                            pyper, c2);
                 cc = make_uint2(c2[0], c2[1]);
             }
             cring[((i + CR - 1) & (CR - 1)) * 32 + lane] = cc;
@@ -486,7 +534,12 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
             float2 g[9];
             pull2(S, O, N, g);
             float2 r_, u_, v_;
-            if (fast) {
+            // pre-collision storage: the last level only streams (its result is the
+            // canonical state); u, v, rho are the moments of that state
+            constexpr bool STREAM_ONLY = PRE && t == T;
+            if (fast && STREAM_ONLY) {
+                moments_pair(g, r_, u_, v_);
+            } else if (fast) {
                 collide_two<C>(g, p.k, r_, u_, v_, mc);
             } else {
                 const uint2 cc = cring[((i - t + CR) & (CR - 1)) * 32 + lane];
@@ -502,7 +555,9 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
                     g[q].x = ((cc.x >> q) & 1u) ? bx : g[q].x;
                     g[q].y = ((cc.y >> q) & 1u) ? by : g[q].y;
                 }
-                if (win_inlet) {
+                if constexpr (STREAM_ONLY) {
+                    moments_pair(g, r_, u_, v_);
+                } else if (win_inlet) {
                     const int R = yk - t;
                     const float lu = inlet_u(p.k, pyper ? wrap(R, p.H) : R);
                     if constexpr (C::MLP) {
@@ -527,7 +582,7 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
                 } else {
                     collide_two<C>(g, p.k, r_, u_, v_, mc);
                 }
-                if (C::MODE == MODE_CORE4) {
+                if (C::MODE != MODE_GENERAL) {
                     // cells that are not updated pass their values on (lbm_core4.cu's
                     // fluid rows 0 and H-1 are read by their neighbours).  With the
                     // general rules a cell that is not updated is solid, out of the
@@ -570,7 +625,7 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
         if (RT >= ya && RT < yb) {
             E *fo = reinterpret_cast<E *>(p.f_out) + (long long)RT * p.pitch + x;
             if (fast) {
-                if (core0) {
+                if (core0 && x + 1 < rx1) {
 #pragma unroll
                     for (int q = 0; q < 9; ++q)
                         st2(fo + q * p.plane, out[q], q);
@@ -590,9 +645,10 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
 #pragma unroll
                 for (int n = 0; n < 2; ++n) {
                     const int xn = x + n;
-                    const bool incore = core0 && xn < p.W;
+                    const bool incore = core0 && xn < rx1;
                     const bool upd = !(cd[n] & C_SKIP);
-                    const bool wr = incore && (upd || (cd[n] & C_GHOST_SKIP));
+                    // lbm_core_smemaa.cu stores every cell (solid ones unchanged)
+                    const bool wr = incore && (upd || (cd[n] & C_GHOST_SKIP) || C::MODE == MODE_PRE_SMEMAA);
                     if (wr) {
 #pragma unroll
                         for (int q = 0; q < 9; ++q)
@@ -685,6 +741,11 @@ template <class C> int rwave_occupancy()
 template <class C> int launch_rwave(WaveParams p, cudaStream_t s)
 {
     const int occ = rwave_occupancy<C>(); // also raises the dynamic shared-memory limit
+    // output rectangle (the whole domain unless set); its x bounds are even
+    const int Wr = p.rx1 > 0 ? p.rx1 - p.rx0 : p.W;
+    const int Hr = p.ry1 > 0 ? p.ry1 - p.ry0 : p.H;
+    if (p.rx1 > 0 && ((p.rx0 | p.rx1) & 1))
+        return LBM_ERR_ARG;
     if (p.chunk <= 0) {
         // Tuning override for experiments: LBM_RW_CHUNK=<rows per item>.
         int v = 0;
@@ -696,13 +757,13 @@ template <class C> int launch_rwave(WaveParams p, cudaStream_t s)
             // 4096 x 1024 cylinder channel: 16 rows at T = 2, 24 at T >= 4); fewer
             // items than resident warps only on small domains.
             v = C::T <= 2 ? 16 : 24;
-            const int nwin = (p.W + C::CW - 1) / C::CW;
+            const int nwin = (Wr + C::CW - 1) / C::CW;
             const long long slots = (long long)sm_count() * occ * C::NW;
-            if ((long long)nwin * ((p.H + v - 1) / v) < slots) {
+            if ((long long)nwin * ((Hr + v - 1) / v) < slots) {
                 long long nch = slots / nwin;
                 if (nch < 1)
                     nch = 1;
-                v = (int)((p.H + nch - 1) / nch);
+                v = (int)((Hr + nch - 1) / nch);
                 if (v < 4 * C::T)
                     v = 4 * C::T;
             }
@@ -718,7 +779,7 @@ template <class C> int launch_rwave(WaveParams p, cudaStream_t s)
         !make_map_mask(&tmm, p.mask, p.W, p.H, p.mask_pitch, C::BWM))
         return LBM_ERR_DEVICE;
     p.use_tma = 1;
-    const RwItems it = rw_items(p.W, p.H, C::CW, C::PADL, p.chunk);
+    const RwItems it = rw_items(Wr, Hr, C::CW, C::PADL, p.chunk);
     const int grid = (it.n_items + C::NW - 1) / C::NW;
     rwave_kernel<C><<<grid, 32 * C::NW, C::SMEM, s>>>(p, tmf, tmm);
     return status(cudaGetLastError());

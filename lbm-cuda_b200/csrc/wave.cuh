@@ -44,6 +44,13 @@ enum : uint32_t {
 enum : int {
     MODE_CORE4 = 0,   // lbm_core4.cu boundary rules
     MODE_GENERAL = 1, // lbm_params boundary rules
+    // Pre-collision storage (the AA kernels' canonical state): collide, then
+    // stream; interior of the domain only (register wavefront kernel).  SMEMAA
+    // writes every cell (solid ones unchanged) and u, v, rho of the fluid ones
+    // (lbm_core_smemaa.cu:500-546); POLICY writes the fluid cells only
+    // (lbm_core_smemaa_policy.cu:338-424).
+    MODE_PRE_SMEMAA = 2,
+    MODE_PRE_POLICY = 3,
 };
 
 struct WaveParams {
@@ -60,6 +67,7 @@ struct WaveParams {
     int use_tma;        // 1: TMA row loads; 0: plain loads (any alignment)
     int *err;           // device error word (bit 0: a bounded wait gave up)
     Phys k;
+    int rx0, rx1, ry0, ry1; // register wavefront: output rectangle (0, W, 0, H when 0, 0, 0, 0)
 };
 
 template <int T_, int NX_, class Ph_, class St_, int MODE_, bool LID_ = false> struct WaveCfg {

@@ -5,6 +5,7 @@ Tolerance: relative L2 error <= 1e-5 (helpers.REL_TOL) on u, v, rho and the
 populations, FP32 with -use_fast_math on both GPU sides."""
 import numpy as np
 import pytest
+import torch
 
 import lbm_b200 as L
 import oracle as O
@@ -222,3 +223,37 @@ def test_refcompat_module_shape():
     assert rel_l2(host(b), ref) < REL_TOL
     pol = L.RefCompatModule("policy")
     assert pol.T == 6 and pol.get_function("macro_kernel") is not None
+
+
+@pytest.mark.parametrize("kind", ["smemaa", "policy"])
+@pytest.mark.parametrize("T", [2, 4, 6])
+def test_split_launch_matches_tile_kernel(kind, T):
+    """lbm_smemaa_step / lbm_blocked_step on TMA-aligned buffers run the AA tile
+    kernel on the edge band and the register wavefront (pre-collision mode) inside;
+    the result must equal the tile kernel everywhere (LBM_AA_SPLIT=0)."""
+    import os
+
+    W, H, n = 2048, 2048, 2  # the split runs on domains of at least 4 M cells
+    m = I.random_discs_mask(W, H, 12, 3.0, 12.0, 21)
+    f0 = I.perturbed_state(W, H, 22, amp=0.02)
+    outs = []
+    for split in ("1", "0"):
+        os.environ["LBM_AA_SPLIT"] = split
+        try:
+            a, b = dev(f0), dev(f0)
+            mac = [torch.zeros((H, W), device="cuda") for _ in range(3)]
+            for _ in range(n):
+                if kind == "smemaa":
+                    L.smemaa_step(dev(m), a, b, *mac, W, H, 1.7, 0.1, T=T)
+                else:
+                    L.blocked_step(dev(m), a, b, W, H, 1.7, 0.1, T=T)
+                a, b = b, a
+            torch.cuda.synchronize()
+            outs.append((host(a), [host(x) for x in mac]))
+        finally:
+            os.environ.pop("LBM_AA_SPLIT", None)
+    (fs, ms), (ft, mt) = outs
+    assert rel_l2(fs, ft) < 1e-6
+    if kind == "smemaa":
+        for x, y in zip(ms, mt):
+            assert rel_l2(x, y) < 1e-6
