@@ -20,6 +20,9 @@ reference does (lbm_mine2.py:106).
 
 --workload batch times 256 independent channel domains of uneven size in one
 persistent launch per T steps (FP16 storage) against one launch per domain.
+--workload c3 runs the 8192 x 2048 cylinder (D = 256, Re = 20 000) in FP32, FP16
+and BF16 deviation storage to 1k / 10k / 50k steps and reports the 16-bit runs'
+velocity error against the FP32 run, and each format's MLUPS at that size.
 --workload dropins times the drop-in entry points for the reference's three
 kernels (lbm_smemaa_step T=4, lbm_blocked_step T=6, lbm_core4_step) and the
 general solver's BGK path at the drivers' 2048 x 512 and at 4096 x 1024; with
@@ -181,7 +184,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32",
                     help="population storage of the cylinder workload (16-bit: deviations f - w)")
-    ap.add_argument("--workload", choices=["cylinder", "batch", "dropins"], default="cylinder")
+    ap.add_argument("--workload", choices=["cylinder", "batch", "dropins", "c3"], default="cylinder")
     ap.add_argument("--closure", choices=["smag", "mlp"], default="smag",
                     help="mlp: the learned closure (random-initialised weights of the 5-32-32-1 network, "
                          "no reference clamps) in place of Smagorinsky")
@@ -223,9 +226,11 @@ def main():
     from lbm_b200 import solver as SV
     from lbm_b200.solver import Solver
 
-    if args.workload in ("batch", "dropins"):
+    if args.workload in ("batch", "dropins", "c3"):
         if args.workload == "batch":
             line = run_batch(args, torch, rank, world, barrier, max_over_ranks)
+        elif args.workload == "c3":
+            line = run_c3(args, torch)
         else:
             line = run_dropins(args, torch, False)
         if rank == 0:
@@ -431,6 +436,54 @@ def run_batch(args, torch, rank, world, barrier, max_over_ranks):
         "gpu_launches": args.steps * ((steps_per + T - 1) // T),
         "clocks": clk.summary(),
     }
+
+
+def run_c3(args, torch):
+    """8192 x 2048 channel past a D = 256 cylinder at (2048, 1024), Re = 20 000
+    (u = 0.05, nu = 6.4e-4, Cs = 0.1), FP32 / FP16 / BF16 storage, T = 2."""
+    from lbm_b200 import init as I
+    from lbm_b200 import solver as SV
+
+    Wc, Hc = 8192, 2048
+    mask = torch.from_numpy(I.cylinder_mask(Wc, Hc, 2048, 1024, 256, value=I.OBSTACLE)).cuda()
+    f0 = torch.from_numpy(I.channel_state(Wc, Hc, u0=0.0, noise=1e-4, seed=0)).cuda()
+    marks = [1000, 10000, 50000] if args.steps >= 3 else [1000]
+    T = 2
+    vel, mlups = {}, {}
+    for name, st in (("f32", SV.STORE_F32), ("f16", SV.STORE_F16DEV), ("bf16", SV.STORE_BF16DEV)):
+        S = SV.Solver(Wc, Hc, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU, storage=st)
+        a = S.new_state()
+        SV.convert_state(f0, SV.STORE_F32, a, st)
+        b = torch.empty_like(a)
+        mac = [torch.empty((Hc, Wc), device="cuda") for _ in range(3)]
+        done, vel[name] = 0, []
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = 0.0
+        for mk in marks:
+            e0.record()
+            which = S.run(a, b, mask, mk - done, T, *mac)
+            e1.record()
+            torch.cuda.synchronize()
+            ms += e0.elapsed_time(e1)
+            if which:
+                a, b = b, a
+            done = mk
+            vel[name].append(torch.stack([mac[0], mac[1]]).cpu())
+        mlups[name] = round(Wc * Hc * done / (ms * 1e3), 1)
+        del S, a, b
+    fl = (mask == 0).cpu()
+    err = {}
+    for name in ("f16", "bf16"):
+        err[name] = []
+        for v, r in zip(vel[name], vel["f32"]):
+            d = (v - r)[:, fl].double()
+            err[name].append(float(d.norm() / r[:, fl].double().norm()))
+    return {"metric": "MLUPS", "value": mlups["f16"], "unit": "MLUPS", "n_gpus": 1, "steps": marks[-1],
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f16-deviation storage, f32 math", "data": "synthetic",
+            "config": {"workload": f"cylinder channel {Wc}x{Hc}, D=256 at (2048,1024), Re=20000, Cs={CS}, "
+                                   f"u={U_IN}, T={T}", "checkpoints": marks},
+            "mlups_by_storage": mlups, "velocity_rel_l2_vs_f32": err}
 
 
 def run_dropins(args, torch, ref):
