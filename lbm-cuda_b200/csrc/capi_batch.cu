@@ -1,8 +1,11 @@
-// Batched independent domains: one persistent launch advances every domain T
-// steps.  CTAs (sm_count x occupancy of them) take (domain, strip, row-chunk)
-// work items from a device counter and run the wavefront tile of wave.cuh on
-// each, so domains of uneven size share the GPU without one launch per domain.
-// Launch pairs (ping-pong) are captured once into a CUDA graph and replayed.
+// Batched independent domains: one launch advances every domain T steps, so
+// domains of uneven size share the GPU without one launch per domain.  Two
+// engines: when every domain is TMA-aligned (and T is 1, 2 or 4), the register
+// wavefront kernel runs one warp per (domain, window, row range) item of a
+// host-built list (edge windows first); otherwise a persistent kernel whose CTAs
+// take (domain, strip, row-chunk) items from a device counter and run the
+// shared-memory wavefront tile of wave.cuh.  Launch pairs (ping-pong) are
+// captured once into a CUDA graph and replayed.
 #include <stdlib.h>
 #include <string.h>
 
@@ -15,8 +18,84 @@ namespace lbm {
 struct __align__(64) BatchDomain {
     CUtensorMap tmf[2]; // input map when f_a (0) / f_b (1) is the source
     CUtensorMap tmm;
+    CUtensorMap rtmf[2]; // the same for the register wavefront's row boxes
+    CUtensorMap rtmm;
     WaveParams p;
     void *f[2];
+    int rw; // 1: the register wavefront can run this domain (TMA-aligned, x not periodic)
+};
+
+// Register-wavefront batch: one warp per (domain, window, row range) item of a
+// host-built list; every domain's inlet / outlet windows come first (see rw_items).
+template <class C>
+__global__ void __launch_bounds__(32 * C::NW, C::MINB)
+    rbatch_kernel(const BatchDomain *__restrict__ doms, const int4 *__restrict__ items, int n_items, int parity)
+{
+    const int it = blockIdx.x * C::NW + (threadIdx.x >> 5);
+    if (it >= n_items)
+        return;
+    const int4 item = items[it]; // domain, window, ya, yb
+    const BatchDomain &d = doms[item.x];
+    WaveParams p = d.p;
+    p.f_in = d.f[parity];
+    p.f_out = d.f[parity ^ 1];
+    rwave_run<C>(p, &d.rtmf[parity], &d.rtmm, item.y, item.z, item.w);
+}
+
+template <class Ph, class St, int T> using RBCfg = RwCfg<T, 1, (T <= 2 ? 1 : 2), Ph, St, MODE_GENERAL>;
+
+template <class C> static int rbatch_launch(const BatchDomain *d, const int4 *items, int n_items, int parity,
+                                            cudaStream_t s)
+{
+    static int attr[64] = {0};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && !attr[dev]) {
+        cudaFuncSetAttribute(rbatch_kernel<C>, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM);
+        attr[dev] = 1;
+    }
+    if (n_items < 1)
+        return LBM_OK;
+    rbatch_kernel<C><<<(n_items + C::NW - 1) / C::NW, 32 * C::NW, C::SMEM, s>>>(d, items, n_items, parity);
+    return status(cudaGetLastError());
+}
+
+template <template <class> class F, class... A> static int with_rcfg(int clamps, int storage, int T, A &&...a)
+{
+    auto go = [&](auto ph, auto st) -> int {
+        using Ph = decltype(ph);
+        using St = decltype(st);
+        switch (T) {
+        case 1:
+            return F<RBCfg<Ph, St, 1>>::run(a...);
+        case 2:
+            return F<RBCfg<Ph, St, 2>>::run(a...);
+        case 4:
+            return F<RBCfg<Ph, St, 4>>::run(a...);
+        default:
+            return LBM_ERR_UNSUPPORTED;
+        }
+    };
+    if (storage == LBM_STORE_F32)
+        return clamps ? go(PhysMrtSmagClamp{}, StoreF32{}) : go(PhysMrtSmag{}, StoreF32{});
+    if (storage == LBM_STORE_F16DEV)
+        return clamps ? go(PhysMrtSmagClamp{}, StoreF16Dev{}) : go(PhysMrtSmag{}, StoreF16Dev{});
+    return LBM_ERR_UNSUPPORTED;
+}
+
+template <class C> struct RLaunchOp {
+    static int run(const BatchDomain *d, const int4 *items, int n_items, int parity, cudaStream_t s)
+    {
+        return rbatch_launch<C>(d, items, n_items, parity, s);
+    }
+};
+template <class C> struct RGeomOp {
+    static int run(int *cw, int *padl)
+    {
+        *cw = C::CW;
+        *padl = C::PADL;
+        return LBM_OK;
+    }
 };
 
 constexpr int kBatchNX = 128;
@@ -129,12 +208,18 @@ template <class C> struct RwOp {
         return LBM_OK;
     }
 };
-template <class C> struct SeparateOp {
-    static int run(const WaveParams &p, cudaStream_t s)
-    {
-        return launch_wave<C>(p, s);
-    }
-};
+// One launch per domain through the single-domain dispatcher (streaming, register
+// or shared-memory wavefront kernel, whichever fits the domain and T).
+static int separate_launch(int clamps, int storage, const WaveParams &w, int T, cudaStream_t s)
+{
+    if (storage == LBM_STORE_F32)
+        return clamps ? launch_step<PhysMrtSmagClamp, StoreF32, MODE_GENERAL>(w, T, s)
+                      : launch_step<PhysMrtSmag, StoreF32, MODE_GENERAL>(w, T, s);
+    if (storage == LBM_STORE_F16DEV)
+        return clamps ? launch_step<PhysMrtSmagClamp, StoreF16Dev, MODE_GENERAL>(w, T, s)
+                      : launch_step<PhysMrtSmag, StoreF16Dev, MODE_GENERAL>(w, T, s);
+    return LBM_ERR_UNSUPPORTED;
+}
 
 } // namespace lbm
 
@@ -152,6 +237,9 @@ struct lbm_batch {
     int cur_T = 0, cur_chunk = 0; // configuration the device item list holds
     std::vector<int4> h_items;
     int tuned_T = 4, tuned_chunk = 64;
+    bool rw_all = false; // every domain can take the register wavefront
+    int cur_engine = 0;  // engine the device item list is for: 0 shared-memory wavefront, 1 register
+    int tuned_engine = 0;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t exec = nullptr;
     int exec_T = 0, exec_chunk = 0;
@@ -159,7 +247,7 @@ struct lbm_batch {
 
 static int batch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
 {
-    if (b->cur_T == T && b->cur_chunk == chunk)
+    if (b->cur_engine == 0 && b->cur_T == T && b->cur_chunk == chunk)
         return LBM_OK;
     int cw = 0;
     int rc = with_cfg<CwOp>(b->p.ref_clamps, b->p.storage, T, &cw);
@@ -192,8 +280,71 @@ static int batch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
     return LBM_OK;
 }
 
+static bool rw_engine(const lbm_batch *b, int T)
+{
+    return b->rw_all && (T == 1 || T == 2 || T == 4);
+}
+
+// Item list of the register wavefront for (T, chunk): the edge windows of every
+// domain first (half-height items), then all other windows.
+static int rbatch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
+{
+    if (b->cur_engine == 1 && b->cur_T == T && b->cur_chunk == chunk)
+        return LBM_OK;
+    int cw = 0, padl = 0;
+    int rc = with_rcfg<RGeomOp>(b->p.ref_clamps, b->p.storage, T, &cw, &padl);
+    if (rc)
+        return rc;
+    b->h_items.clear();
+    std::vector<int4> mid;
+    for (int d = 0; d < (int)b->doms.size(); ++d) {
+        const RwItems it = rw_items(b->doms[d].W, b->doms[d].H, cw, padl, chunk);
+        for (int i = 0; i < it.n_items; ++i) {
+            int win, ya, yb;
+            rw_item(it, i, b->doms[d].H, chunk, win, ya, yb);
+            (i < it.n_edge_items ? b->h_items : mid).push_back(make_int4(d, win, ya, yb));
+        }
+    }
+    b->h_items.insert(b->h_items.end(), mid.begin(), mid.end());
+    if ((int)b->h_items.size() > b->max_items)
+        return LBM_ERR_ARG;
+    cudaError_t e = cudaMemcpyAsync(b->d_items, b->h_items.data(), sizeof(int4) * b->h_items.size(),
+                                    cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_doms, b->hdoms.data(), sizeof(BatchDomain) * b->hdoms.size(),
+                            cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess)
+        return status(e);
+    b->n_items = (int)b->h_items.size();
+    b->cur_T = T;
+    b->cur_chunk = chunk;
+    b->cur_engine = 1;
+    return LBM_OK;
+}
+
+static int prepare(lbm_batch *b, int T, int chunk, cudaStream_t s)
+{
+    if (rw_engine(b, T))
+        return rbatch_items(b, T, chunk, s);
+    if (b->cur_engine != 0) {
+        b->cur_T = 0; // force a rebuild of the shared-memory wavefront's list
+        b->cur_engine = 0;
+    }
+    return batch_items(b, T, chunk, s);
+}
+
+static bool prepared(const lbm_batch *b, int T, int chunk)
+{
+    return b->cur_T == T && b->cur_chunk == chunk && b->cur_engine == (rw_engine(b, T) ? 1 : 0);
+}
+
 static int batch_launch_one(lbm_batch *b, int T, int parity, cudaStream_t s)
 {
+    if (rw_engine(b, T))
+        return with_rcfg<RLaunchOp>(b->p.ref_clamps, b->p.storage, T, (const BatchDomain *)b->d_doms,
+                                    (const int4 *)b->d_items, b->n_items, parity, s);
     return with_cfg<LaunchOp>(b->p.ref_clamps, b->p.storage, T, (const BatchDomain *)b->d_doms,
                               (const int4 *)b->d_items, b->n_items, b->d_counter, parity, s);
 }
@@ -261,10 +412,22 @@ int lbm_batch_create(const lbm_params *common, const lbm_domain *domains, int n,
                   make_map_planes(&hd.tmf[1], dm.f_b, es, dm.W, dm.H, dm.pitch, w.plane, rw) &&
                   make_map_mask(&hd.tmm, dm.mask, dm.W, dm.H, dm.mask_pitch, rwm);
         w.use_tma = tma ? 1 : 0;
-        // bound on the work items of any (T, chunk >= 8) configuration
-        max_items += ((dm.W + (kBatchNX - 16) - 1) / (kBatchNX - 16)) * ((dm.H + 7) / 8);
+        // register wavefront: row boxes of 64 + 16 / es elements and 80 mask bytes
+        hd.rw = tma && make_map_planes(&hd.rtmf[0], dm.f_a, es, dm.W, dm.H, dm.pitch, w.plane, 64 + 16 / es) &&
+                make_map_planes(&hd.rtmf[1], dm.f_b, es, dm.W, dm.H, dm.pitch, w.plane, 64 + 16 / es) &&
+                make_map_mask(&hd.rtmm, dm.mask, dm.W, dm.H, dm.mask_pitch, 80);
+        // bound on the work items of any (T, chunk >= 8) configuration of either engine
+        max_items += ((dm.W + (kBatchNX - 16) - 1) / (kBatchNX - 16)) * ((dm.H + 7) / 8) +
+                     ((dm.W + 51) / 52) * ((dm.H + 3) / 4);
     }
     b->max_items = max_items;
+    b->rw_all = true;
+    for (const auto &hd : b->hdoms)
+        b->rw_all = b->rw_all && hd.rw;
+    if (b->rw_all) {
+        b->tuned_T = 2;
+        b->tuned_chunk = 16;
+    }
     cudaError_t e = cudaMalloc(&b->d_doms, sizeof(BatchDomain) * n);
     if (e == cudaSuccess)
         e = cudaMalloc(&b->d_items, sizeof(int4) * max_items);
@@ -308,10 +471,10 @@ int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cs);
     const bool capturing = cs != cudaStreamCaptureStatusNone;
-    if (!(b->cur_T == T && b->cur_chunk == chunk)) {
+    if (!prepared(b, T, chunk)) {
         if (capturing)
             return LBM_ERR_ARG; // the item list must be prepared outside a capture (run once first)
-        int rc = batch_items(b, T, chunk, s);
+        int rc = prepare(b, T, chunk, s);
         if (rc)
             return rc;
     }
@@ -354,10 +517,10 @@ int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in
         // remaining steps: launches of depth T, then the largest supported depth that fits
         const int left = n_steps - done;
         const int t = left >= T ? T : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
-        if (t != b->cur_T) {
+        if (!prepared(b, t, chunk)) {
             if (capturing)
                 return LBM_ERR_ARG;
-            int rc = batch_items(b, t, chunk, s);
+            int rc = prepare(b, t, chunk, s);
             if (rc)
                 return rc;
         }
@@ -387,7 +550,7 @@ int lbm_batch_run_separate(lbm_batch *b, int n_steps, int T, void *stream, int *
             w.f_in = b->hdoms[d].f[parity];
             w.f_out = b->hdoms[d].f[parity ^ 1];
             w.chunk = 0;
-            int rc = with_cfg<SeparateOp>(b->p.ref_clamps, b->p.storage, t, w, s);
+            int rc = separate_launch(b->p.ref_clamps, b->p.storage, w, t, s);
             if (rc)
                 return rc;
         }
@@ -405,7 +568,7 @@ int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk)
         return LBM_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int Ts[] = {1, 2, 4, 8};
-    const int chunks[] = {16, 32, 64, 128};
+    const int chunks[] = {8, 16, 24, 32, 64, 128};
     float best = 1e30f;
     int bT = 4, bC = 64;
     cudaEvent_t e0, e1;
@@ -413,9 +576,9 @@ int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk)
     cudaEventCreate(&e1);
     for (int T : Ts) {
         for (int ch : chunks) {
-            if (ch < 2 * T)
+            if (ch < 2 * T || (rw_engine(b, T) ? ch > 32 : ch < 16))
                 continue;
-            int rc = batch_items(b, T, ch, s);
+            int rc = prepare(b, T, ch, s);
             if (rc)
                 return rc;
             for (int w = 0; w < 2; ++w)

@@ -332,33 +332,26 @@ __device__ __forceinline__ void collide_two(float2 (&g)[9], const Phys &k, float
     }
 }
 
+// One work item: window `win` (columns rx0 + win CW - PADL ..) and output rows
+// [ya, yb) of the domain p; run by one whole warp (lane = threadIdx.x % 32, the
+// warp's shared memory at wi * WARP_BYTES).
 template <class C>
-__global__ void __launch_bounds__(32 * C::NW, C::MINB)
-    rwave_kernel(const __grid_constant__ WaveParams p, const __grid_constant__ CUtensorMap tmf,
-                 const __grid_constant__ CUtensorMap tmm)
+__device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap *tmf_, const CUtensorMap *tmm_,
+                                          int win, int ya, int yb)
 {
     using Ph = typename C::Ph;
     using St = typename C::St;
     using E = typename C::E;
     constexpr int T = C::T, D = C::D, P = C::P, BW = C::BW, CR = C::CR;
     constexpr unsigned M = 0xffffffffu;
+    constexpr bool PRE = C::MODE == MODE_PRE_SMEMAA || C::MODE == MODE_PRE_POLICY;
+    const CUtensorMap &tmf = *tmf_;
+    const CUtensorMap &tmm = *tmm_;
 
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31;
     const int wi = threadIdx.x >> 5;
-    constexpr bool PRE = C::MODE == MODE_PRE_SMEMAA || C::MODE == MODE_PRE_POLICY;
-    // output rectangle [rx0, rx1) x [ry0, ry1) (the whole domain unless set)
     const int rx0 = p.rx1 > 0 ? p.rx0 : 0, rx1 = p.rx1 > 0 ? p.rx1 : p.W;
-    const int ry0 = p.ry1 > 0 ? p.ry0 : 0, ry1 = p.ry1 > 0 ? p.ry1 : p.H;
-    const RwItems items = rw_items(rx1 - rx0, ry1 - ry0, C::CW, C::PADL, p.chunk);
-    const int item = blockIdx.x * C::NW + wi;
-    if (item >= items.n_items)
-        return; // whole warp: no item left (nothing below waits on other warps)
-    int win, ya, yb;
-    rw_item(items, item, ry1 - ry0, p.chunk, win, ya, yb);
-    ya += ry0;
-    yb += ry0;
-
     unsigned char *wbase = smem + wi * C::WARP_BYTES;
     uint64_t *bar = reinterpret_cast<uint64_t *>(wbase);
     unsigned char *ring = wbase + 128;
@@ -698,6 +691,23 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
         }
         __syncwarp();
     }
+}
+
+template <class C>
+__global__ void __launch_bounds__(32 * C::NW, C::MINB)
+    rwave_kernel(const __grid_constant__ WaveParams p, const __grid_constant__ CUtensorMap tmf,
+                 const __grid_constant__ CUtensorMap tmm)
+{
+    // output rectangle [rx0, rx1) x [ry0, ry1) (the whole domain unless set)
+    const int rx0 = p.rx1 > 0 ? p.rx0 : 0, rx1 = p.rx1 > 0 ? p.rx1 : p.W;
+    const int ry0 = p.ry1 > 0 ? p.ry0 : 0, ry1 = p.ry1 > 0 ? p.ry1 : p.H;
+    const RwItems items = rw_items(rx1 - rx0, ry1 - ry0, C::CW, C::PADL, p.chunk);
+    const int item = blockIdx.x * C::NW + (threadIdx.x >> 5);
+    if (item >= items.n_items)
+        return; // whole warp: no item left (nothing below waits on other warps)
+    int win, ya, yb;
+    rw_item(items, item, ry1 - ry0, p.chunk, win, ya, yb);
+    rwave_run<C>(p, &tmf, &tmm, win, ya + ry0, yb + ry0);
 }
 
 // Launch constraints: TMA-aligned planes and mask (16-byte base, pitches and
