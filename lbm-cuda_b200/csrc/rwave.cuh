@@ -43,12 +43,20 @@
 namespace lbm {
 
 template <int T_, int NW_, int P_, class Ph_, class St_, int MODE_, bool LID_ = false, bool PACKED_ = true,
-          int MINB_ = 0>
+          int MINB_ = 0, int LAG_ = 1>
 struct RwCfg {
     static constexpr int T = T_;
     static constexpr int NW = NW_; // warps (windows) per CTA
     static constexpr int P = P_;   // TMA prefetch distance in rows
     static constexpr int D = P + 3; // ring depth: rows yk-2, yk-1, yk in use + P in flight
+    // Rows between consecutive time levels: 1 (level t at row yk - t) or 2 (level t
+    // at row yk - 1 - 2 (t - 1): the levels of an iteration no longer depend on
+    // each other, at the cost of one more carried row per level).  Lag 2 passed the
+    // parity tests but measured slower at T = 2 (64 against 113 GLUPS FP32 on the
+    // 4096 x 1024 cylinder: the extra row spills at 128 registers), so the
+    // dispatchers use lag 1.
+    static constexpr int LAG = LAG_;
+    static_assert(LAG == 1 || LAG == 2, "lag");
     // Left pad of the window: T rounded up to even, so that a lane's column pair
     // stays 8-byte aligned; CW output columns [PADL, 64 - PADL).
     static constexpr int PADL = T_ + (T_ & 1);
@@ -73,11 +81,11 @@ struct RwCfg {
     static constexpr int SMEM = NW * WARP_BYTES;
     static constexpr uint32_t TX_BYTES = 9 * BW * ES + BWM;
     // resident warps per SM the registers are sized for: 16 / 12 / 8 (<= 128 / 170 / 255 registers)
-    static constexpr int MINB_R = ((T <= 2 && !MLP) ? 16 : ((T <= 4) ? 12 : 8)) / NW;
+    static constexpr int MINB_R = ((T <= 2 && !MLP) ? (LAG_ == 2 ? 14 : 16) : ((T <= 4) ? 12 : 8)) / NW;
     static constexpr int MINB_S = (227 * 1024) / (SMEM + 1024);
     static constexpr int MINB_A = MINB_ > 0 ? MINB_ : MINB_R; // blocks per SM the registers are sized for
     static constexpr int MINB = MINB_A < MINB_S ? MINB_A : MINB_S;
-    static_assert(T >= 1 && T <= 6 && CR >= T, "temporal depth");
+    static_assert(T >= 1 && T <= 6 && CR >= LAG_ * (T - 1) + 2, "temporal depth / code ring rows");
     static_assert(D * 8 <= 128, "mbarriers");
     static_assert(MINB >= 1, "shared memory");
 };
@@ -368,7 +376,8 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
     const int xs = rx0 + win * C::CW - C::PADL;
     const int x = xs + 2 * lane; // column of the lane's first cell
     const int row0 = ya - T;
-    const int nrows = yb - ya + 2 * T;
+    constexpr int LAG = C::LAG;
+    const int nrows = yb - ya + T + LAG * (T - 1) + 1;
     const bool pyper = (C::MODE == MODE_GENERAL) && p.bc_y == LBM_BC_PERIODIC;
     const int xa = floor_div(xs, C::AE) * C::AE; // TMA box origins (aligned)
     const int xm = floor_div(xs, 16) * 16;
@@ -416,13 +425,14 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
     // Carried levels 1..T-1: pv = row yk-t-1 (all q), p2 = row yk-t-2 (q 2,5,6
     // stored at their own indices; the others unused), cu = row yk-t.
     constexpr int NL = T > 1 ? T - 1 : 1; // carried levels (one unused slot at T = 1)
-    float2 pv[NL][9], p2[NL][9], cu[NL][9];
+    float2 pv[NL][9], p2[NL][9], p3[NL][9], cu[NL][9]; // p3: the LAG == 2 extra row
 #pragma unroll
     for (int t = 0; t < NL; ++t)
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
             pv[t][q] = make_float2(wgt(q), wgt(q));
             p2[t][q] = pv[t][q];
+            p3[t][q] = pv[t][q];
             cu[t][q] = pv[t][q];
         }
 
@@ -500,13 +510,19 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
             cring[((i + CR - 1) & (CR - 1)) * 32 + lane] = cc;
         }
 
-        const bool fast = (hist & ((1u << T) - 1u)) == 0u;
+        constexpr uint32_t HMASK = [] {
+            uint32_t m = 0;
+            for (int t = 1; t <= C::T; ++t)
+                m |= 1u << (C::LAG * (t - 1));
+            return m;
+        }();
+        const bool fast = (hist & HMASK) == 0u;
         float2 out[9], mr, mu, mv;
 
         // Level t: sources S/O/N of level t-1, result into cu[t-1] (t < T) or out.
         static_for<1, T + 1>([&](auto tt) {
             constexpr int t = decltype(tt)::value;
-            if (i < 2 * t)
+            if (i < 1 + t + LAG * (t - 1))
                 return; // below level t's cone: nothing valid to compute yet
             float2 S[9], O[9], N[9];
             if constexpr (t == 1) {
@@ -519,9 +535,15 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
             } else {
 #pragma unroll
                 for (int q = 0; q < 9; ++q) {
-                    S[q] = p2[t - 2][q];
-                    O[q] = pv[t - 2][q];
-                    N[q] = cu[t - 2][q];
+                    if constexpr (LAG == 1) {
+                        S[q] = p2[t - 2][q];
+                        O[q] = pv[t - 2][q];
+                        N[q] = cu[t - 2][q];
+                    } else {
+                        S[q] = p3[t - 2][q];
+                        O[q] = p2[t - 2][q];
+                        N[q] = pv[t - 2][q];
+                    }
                 }
             }
             float2 g[9];
@@ -535,7 +557,7 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
             } else if (fast) {
                 collide_two<C>(g, p.k, r_, u_, v_, mc);
             } else {
-                const uint2 cc = cring[((i - t + CR) & (CR - 1)) * 32 + lane];
+                const uint2 cc = cring[((i - 1 - LAG * (t - 1) + 2 * CR) & (CR - 1)) * 32 + lane];
                 // half-way bounce-back (and Ladd's moving-wall term) by selects
 #pragma unroll
                 for (int q = 1; q < 9; ++q) {
@@ -551,7 +573,7 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
                 if constexpr (STREAM_ONLY) {
                     moments_pair(g, r_, u_, v_);
                 } else if (win_inlet) {
-                    const int R = yk - t;
+                    const int R = yk - 1 - LAG * (t - 1);
                     const float lu = inlet_u(p.k, pyper ? wrap(R, p.H) : R);
                     if constexpr (C::MLP) {
                         collide_pair_mlp<Ph, true>(g, (cc.x & C_INLET) != 0, (cc.y & C_INLET) != 0, lu, p.k, mc.F,
@@ -614,7 +636,7 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
         });
 
         // ---- level T: store row yk - T ----
-        const int RT = yk - T;
+        const int RT = yk - 1 - LAG * (T - 1);
         if (RT >= ya && RT < yb) {
             E *fo = reinterpret_cast<E *>(p.f_out) + (long long)RT * p.pitch + x;
             if (fast) {
@@ -633,7 +655,7 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
                     }
                 }
             } else {
-                const uint2 cc = cring[((i - T + CR) & (CR - 1)) * 32 + lane];
+                const uint2 cc = cring[((i - 1 - LAG * (T - 1) + 2 * CR) & (CR - 1)) * 32 + lane];
                 const uint32_t cd[2] = {cc.x, cc.y};
 #pragma unroll
                 for (int n = 0; n < 2; ++n) {
@@ -660,9 +682,18 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
         // ---- rotate the carried rows ----
 #pragma unroll
         for (int t = 0; t < T - 1; ++t) {
-            p2[t][2] = pv[t][2];
-            p2[t][5] = pv[t][5];
-            p2[t][6] = pv[t][6];
+            if constexpr (LAG == 2) {
+                p3[t][2] = p2[t][2];
+                p3[t][5] = p2[t][5];
+                p3[t][6] = p2[t][6];
+#pragma unroll
+                for (int q = 0; q < 9; ++q)
+                    p2[t][q] = pv[t][q];
+            } else {
+                p2[t][2] = pv[t][2];
+                p2[t][5] = pv[t][5];
+                p2[t][6] = pv[t][6];
+            }
 #pragma unroll
             for (int q = 0; q < 9; ++q)
                 pv[t][q] = cu[t][q];
