@@ -80,8 +80,7 @@ template <int T_, int VAR_, int SX_ = 64, int SY_ = 32, int NT_ = 256, int NB_ =
     static constexpr int OFF_M = OFF_F + 9 * PL * 4;
     static constexpr int OFF_C = OFF_M + round_up(MW * SY, 128);
     static constexpr int OFF_LU = OFF_C + SX * SY * 2;
-    static constexpr int OFF_DUM = OFF_LU + SY * 4;
-    static constexpr int SMEM = OFF_DUM + 9 * NT * 4;
+    static constexpr int SMEM = OFF_LU + SY * 4;
     static constexpr int BATCH = NB_;
     static_assert(ROWS_PER_THREAD % NB_ == 0, "batch");
     static constexpr uint32_t TX = 9 * PL * 4 + MW * SY;
@@ -194,7 +193,6 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
 
     // Inlet velocity of each tile row (only the tile holding column 0 uses it).
     float *lu_row = reinterpret_cast<float *>(smem + C::OFF_LU);
-    float *dummy = reinterpret_cast<float *>(smem + C::OFF_DUM) + tid; // per-thread write-only sink
     if (tid < SY)
         lu_row[tid] = inlet_u(p.k, yt + tid);
     __syncthreads();
@@ -230,7 +228,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
                 const int r = rb + RS * (b + jj), c = col;
 #pragma unroll
                 for (int q = 0; q < 9; ++q)
-                    *(act[jj] ? &sl(opp(q), c, r) : dummy + q * C::NT) = f[jj][q];
+                    if (act[jj])
+                        sl(opp(q), c, r) = f[jj][q];
             }
         }
     };
@@ -276,7 +275,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
                     const int r = rr_[jj], c = cc_[jj];
 #pragma unroll
                     for (int q = 0; q < 9; ++q)
-                        *(act[jj] ? &sl(q, c + cx(q), r + cy(q)) : dummy + q * C::NT) = f[jj][q];
+                        if (act[jj])
+                            sl(q, c + cx(q), r + cy(q)) = f[jj][q];
                 }
                 continue;
             }
@@ -308,7 +308,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
                         dst = &sl(opp(q), c, r);
                     else
                         dst = &sl(q, c + cx(q), r + cy(q));
-                    *(act[jj] ? dst : dummy + q * C::NT) = f[jj][q];
+                    if (act[jj])
+                        *dst = f[jj][q];
                 }
             }
         }
