@@ -11,7 +11,11 @@ path for this workload; 1 runs the streaming kernel, 3-8 the other temporally
 blocked kernels).
 Synthetic inputs with that shape (there is no external dataset).
 
-One bench "step" is one frame of `--frame` physical steps (default 100).
+One bench "step" is one frame of `--frame` physical steps (default 50, the
+reference driver's 25 graph launches of 2 steps per displayed frame,
+lbm_mine2.py:88-91).  The e2e figure runs that frame through the public API
+with the solid mask uploaded from pinned host memory and the vorticity image
+(RGBA8, W x H x 4 bytes) read back to pinned host memory every frame.
 Metric: MLUPS = W*H*physical steps / time, counting every cell as the
 reference does (lbm_mine2.py:106).
 
@@ -174,13 +178,14 @@ def dist_env():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--steps", type=int, default=150)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--T", type=int, default=2,
                     help="steps fused per launch (1: streaming kernel; 2, 4, 6: register wavefront; 3-8: "
                          "shared-memory wavefront)")
-    ap.add_argument("--frame", type=int, default=100, help="physical steps per bench step")
+    ap.add_argument("--frame", type=int, default=50,
+                    help="physical steps per bench step (50: one display frame of the reference's driver)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32",
                     help="population storage of the cylinder workload (16-bit: deviations f - w)")
@@ -286,40 +291,68 @@ def main():
     ms_per_step = ms / args.steps
     launch_ms = ms / (args.steps * n_launch)
 
-    # End to end through the public API with host buffers: every step uploads
-    # the state and mask from pinned host memory, runs the frame and reads back
-    # u, v, rho of the last step.
-    host_f = f_a.cpu().pin_memory()
-    host_m = torch.from_numpy(mask_np).pin_memory()
-    host_mac = [torch.empty((H, W), dtype=torch.float32).pin_memory() for _ in range(3)]
+    # End to end through the public API with host buffers, one display frame of
+    # the reference's driver per step (lbm_mine2.py:88-95): the frame's steps,
+    # u, v, rho written by the last launch, the vorticity colour map
+    # (lbm_visualize, scale 50) and the RGBA frame read back to pinned host
+    # memory; the solid mask is the step's input, uploaded from pinned host
+    # memory every frame.  The populations stay resident, as in the driver.
+    # Uploads, frames and read-backs run on three streams with two mask and two
+    # image buffers, so frame i+1 computes while frame i's image is copied out.
+    host_m = [torch.from_numpy(mask_np).pin_memory() for _ in range(2)]
+    dev_m = [torch.empty_like(mask) for _ in range(2)]
+    host_img = [torch.empty((H, W, 4), dtype=torch.uint8).pin_memory() for _ in range(2)]
+    dev_img = [torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda") for _ in range(2)]
     dev_mac = [torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in range(3)]
+    up, down = torch.cuda.Stream(), torch.cuda.Stream()
+    ev_up = [torch.cuda.Event() for _ in range(2)]
+    ev_comp = [torch.cuda.Event() for _ in range(2)]
+    ev_down = [torch.cuda.Event() for _ in range(2)]
     e2e_steps = max(3, args.steps // 3)
 
-    def e2e_step():
-        st["a"].copy_(host_f, non_blocking=True)
-        mask.copy_(host_m, non_blocking=True)
+    def e2e_step(i):
+        j = i & 1
+        with torch.cuda.stream(up):
+            up.wait_event(ev_comp[j])  # frame i-2 has finished reading this mask buffer
+            dev_m[j].copy_(host_m[j], non_blocking=True)
+            ev_up[j].record(up)
+        stream.wait_event(ev_up[j])
+        stream.wait_event(ev_down[j])  # frame i-2's image has been copied out
         for li in range(n_launch):
             last = li == n_launch - 1
-            which = S.run(st["a"], st["b"], mask, T, T, *(dev_mac if last else (None, None, None)))
+            which = S.run(st["a"], st["b"], dev_m[j], T, T, *(dev_mac if last else (None, None, None)),
+                          stream=stream)
             if which:
                 st["a"], st["b"] = st["b"], st["a"]
-        for h_, d_ in zip(host_mac, dev_mac):
-            h_.copy_(d_, non_blocking=True)
+        L.visualize(*dev_mac, dev_img[j], dev_m[j], W, H, 50.0, stream=stream)
+        ev_comp[j].record(stream)
+        with torch.cuda.stream(down):
+            down.wait_event(ev_comp[j])
+            host_img[j].copy_(dev_img[j], non_blocking=True)
+            ev_down[j].record(down)
 
-    e2e_step()
+    for j in range(2):  # every event recorded once before the first wait on it
+        ev_comp[j].record(stream)
+        ev_down[j].record(stream)
+    e2e_step(0)
+    e2e_step(1)
     torch.cuda.synchronize()
     barrier()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
     e2.record(stream)
-    for _ in range(e2e_steps):
-        e2e_step()
+    for i in range(e2e_steps):
+        e2e_step(i)
+    for j in range(2):
+        stream.wait_event(ev_down[j])
     e3.record(stream)
     torch.cuda.synchronize()
     e2e_ms = max_over_ranks(e2.elapsed_time(e3))
     e2e_mlups = W * H * e2e_steps * n_launch * T * world / (e2e_ms * 1e3)
-    h2d = host_f.numel() * host_f.element_size() + host_m.numel()
-    d2h = sum(t.numel() * t.element_size() for t in host_mac)
+    h2d = host_m[0].numel() * host_m[0].element_size()
+    d2h = host_img[0].numel() * host_img[0].element_size()
+    if not bool((host_img[(e2e_steps - 1) & 1][1:-1, 1:-1, 3] == 255).all()):  # border cells stay unwritten
+        raise RuntimeError("the read-back frame is not a complete RGBA image")
 
     flags = L.solver.device_error_flags(clear=True)
     if rank == 0:

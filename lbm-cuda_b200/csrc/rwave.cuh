@@ -42,6 +42,10 @@
 
 namespace lbm {
 
+#ifndef LBM_MLP_WARPS
+#define LBM_MLP_WARPS 12 // resident warps per SM the learned-closure kernels are sized for
+#endif
+
 template <int T_, int NW_, int P_, class Ph_, class St_, int MODE_, bool LID_ = false, bool PACKED_ = true,
           int MINB_ = 0, int LAG_ = 1>
 struct RwCfg {
@@ -81,7 +85,8 @@ struct RwCfg {
     static constexpr int SMEM = NW * WARP_BYTES;
     static constexpr uint32_t TX_BYTES = 9 * BW * ES + BWM;
     // resident warps per SM the registers are sized for: 16 / 12 / 8 (<= 128 / 170 / 255 registers)
-    static constexpr int MINB_R = ((T <= 2 && !MLP) ? (LAG_ == 2 ? 14 : 16) : ((T <= 4) ? 12 : 8)) / NW;
+    static constexpr int MINB_R =
+        (MLP ? LBM_MLP_WARPS : ((T <= 2) ? (LAG_ == 2 ? 14 : 16) : ((T <= 4) ? 12 : 8))) / NW;
     static constexpr int MINB_S = (227 * 1024) / (SMEM + 1024);
     static constexpr int MINB_A = MINB_ > 0 ? MINB_ : MINB_R; // blocks per SM the registers are sized for
     static constexpr int MINB = MINB_A < MINB_S ? MINB_A : MINB_S;
