@@ -149,7 +149,13 @@ class HeadlessDriver:
         self.mask = torch.as_tensor(np.asarray(mask, dtype=np.uint8)).to(dev).contiguous()
         f0 = reference_initial_state(W, H) if f0 is None else np.asarray(f0, dtype=np.float32)
         self.f_now = torch.from_numpy(np.ascontiguousarray(f0)).to(dev)
-        self.f_out = torch.empty_like(self.f_now)
+        # f_out starts as a copy of f_now.  The T = 4 / 6 drivers allocate it
+        # uninitialised (cp.empty_like, lbm_smemaa_main.py:44,
+        # lbm_smemaa_endfused_main.py:33) and the AA kernels never write some of
+        # its slots (solid cells, the outlet corners), which then keep whatever
+        # the allocation held; a copy makes every run reproducible (lbm_mine2.py:36
+        # copies too).
+        self.f_out = self.f_now.clone()
         # the drivers pass their initial u, v, rho arrays as the kernels' macro outputs
         self.ux = torch.zeros((H, W), dtype=torch.float32, device=dev)
         self.uy = torch.zeros_like(self.ux)

@@ -5,8 +5,8 @@ Each driver captures the reference drivers' CUDA graph of two launches
 then (end-fused driver) the macro kernel and the colour map.  Checks: the
 graph-replayed frames give exactly the state and image of the same launches
 issued eagerly; the frames agree with the oracle's emulation of the driver loop
-(relative L2 <= 1e-5 on the populations and u, v, rho, image bytes within one
-level); the split launch (edge tiles on a forked stream, register wavefront
+(relative L2 <= 1e-5 on the populations and u, v, rho; the image exact on the
+GPU's u, v and within one level of the oracle's); the split launch (edge tiles on a forked stream, register wavefront
 inside) is captured into the graph correctly; MLUPS follows the drivers'
 formula; PNG output round-trips."""
 import numpy as np
@@ -68,8 +68,10 @@ def test_driver_graph_vs_eager_and_oracle(kind, W, H):
     assert rel_l2(fg, fo) < REL_TOL
     for x, y in zip(mg, mo):
         assert rel_l2(x, y) < REL_TOL
-    diff = np.abs(ig.astype(np.int16) - io.astype(np.int16))
-    assert diff.max() <= 1 and (diff > 0).mean() < 1e-3
+    # the colour map is exact on the GPU's own u, v; against the oracle's frame a
+    # byte may differ by one level (near-zero vorticity sits on a truncation edge)
+    np.testing.assert_array_equal(ig, O.visualize(mg[0], mg[1], mask, D.VORT_SCALE))
+    assert np.abs(ig.astype(np.int16) - io.astype(np.int16)).max() <= 1
 
 
 @pytest.mark.parametrize("kind", ["smemaa", "endfused"])
