@@ -13,12 +13,14 @@
 // solid; out-of-domain cells are solid with zero populations, column W-1 is
 // fluid (open outlet ghost).
 //
-// B200 design: one CTA of 256 threads owns a 64 x 32 tile (core (64-2T) x
+// B200 design: one CTA of 512 threads owns a 64 x 32 tile (core (64-2T) x
 // (32-2T) plus a T-cell halo), fetched by a single TMA box [68 x 32 x 9] (plus
 // one for the mask) when the layout allows it.  Threads have a fixed 2-D map
 // (two warps per tile row, eight rows apart), so phases need no integer
-// division; per-cell neighbour codes are built once after the load, so the B
-// phase reads one 16-bit code instead of nine mask bytes.  Two CTAs fit per SM.
+// division.  After the load the solid test runs once per tile cell and per cell
+// of a one-cell apron (a byte array), and each cell's neighbour code is read
+// off those bytes, so the B phase reads one 16-bit code instead of nine mask
+// bytes.  Two CTAs fit per SM.
 #pragma once
 
 #include "wave.cuh" // IntC
@@ -80,7 +82,9 @@ template <int T_, int VAR_, int SX_ = 64, int SY_ = 32, int NT_ = 256, int NB_ =
     static constexpr int OFF_M = OFF_F + 9 * PL * 4;
     static constexpr int OFF_C = OFF_M + round_up(MW * SY, 128);
     static constexpr int OFF_LU = OFF_C + SX * SY * 2;
-    static constexpr int SMEM = OFF_LU + SY * 4;
+    static constexpr int SBW = SX + 2;             // solid-flag rows: the tile plus a one-cell apron
+    static constexpr int OFF_SB = OFF_LU + round_up(SY * 4, 16);
+    static constexpr int SMEM = OFF_SB + round_up(SBW * (SY + 2), 16);
     static constexpr int BATCH = NB_;
     static_assert(ROWS_PER_THREAD % NB_ == 0, "batch");
     static constexpr uint32_t TX = 9 * PL * 4 + MW * SY;
@@ -158,18 +162,26 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
             return true; // outside the tile: only read for cells whose results are discarded
         return M[r * MW + c + om] != 0;
     };
+    // solid flags of every tile cell and of a one-cell apron around the tile, once
+    constexpr int SBW = C::SBW;
+    uint8_t *SB = smem + C::OFF_SB;
+    for (int e = tid; e < SBW * (SY + 2); e += C::NT)
+        SB[e] = solid(e % SBW - 1, e / SBW - 1) ? 1 : 0;
+    // Inlet velocity of each tile row (only the tile holding column 0 uses it).
+    float *lu_row = reinterpret_cast<float *>(smem + C::OFF_LU);
+    if (tid < SY)
+        lu_row[tid] = inlet_u(p.k, yt + tid);
+    __syncthreads();
 #pragma unroll
     for (int j = 0; j < C::ROWS_PER_THREAD; ++j) {
         const int r = rb + RS * j, c = col;
         const int x = xt + c, y = yt + r;
-        uint16_t cd = 0;
-        if (x >= 0 && x < W - 1 && y > 0 && y < H - 1 && !solid(c, r))
-            cd |= AA_UPD;
+        const uint8_t *sb = SB + (r + 1) * SBW + (c + 1);
+        uint32_t cd = (x >= 0 && x < W - 1 && y > 0 && y < H - 1 && !sb[0]) ? AA_UPD : 0u;
 #pragma unroll
         for (int q = 1; q < 9; ++q)
-            if (solid(c - cx(q), r - cy(q)))
-                cd |= (uint16_t)(1u << q);
-        code[r * SX + c] = cd;
+            cd |= (uint32_t)sb[-cx(q) - cy(q) * SBW] << q;
+        code[r * SX + c] = (uint16_t)cd;
     }
     __syncthreads();
 
@@ -190,12 +202,6 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
         float r, u, v;
         collide<PhysBgkRef>(f, x == 0, y, p.k, r, u, v);
     };
-
-    // Inlet velocity of each tile row (only the tile holding column 0 uses it).
-    float *lu_row = reinterpret_cast<float *>(smem + C::OFF_LU);
-    if (tid < SY)
-        lu_row[tid] = inlet_u(p.k, yt + tid);
-    __syncthreads();
 
     // Cells are processed in batches of C::BATCH rows per thread: all loads,
     // then all collisions, then all stores, so the independent cells overlap.
@@ -405,7 +411,7 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
             f[q] = sl(q, c, r);
             p.f_out[q * N + id] = f[q];
         }
-        if (!solid(c, r) && x < W - 1 && y > 0 && y < H - 1) {
+        if (code[r * SX + c] & AA_UPD) {
             float rr, uu, vv;
             moments_seq(f, rr, uu, vv);
             p.ux[id] = uu;

@@ -68,13 +68,15 @@ template <class C> int launch_aa_grid(AaParams p, int nblocks, cudaStream_t s)
 
 template <class Cfg, int MODE> static int aa_split(AaParams p, int T, cudaStream_t s, bool &done);
 
-// Tile shapes: (SX, SY, threads, cells per batch, CTAs per SM).  Shape 0 is a
-// 64 x 32 tile (less halo recomputation), shape 1 a 32 x 32 tile with more
-// CTAs per SM (more warps to hide latency).
+// Tile shapes: (SX, SY, threads, cells per batch, CTAs per SM).  Shape 2, the
+// default, is a 64 x 32 tile with 512 threads and two CTAs per SM (measured
+// against 32 x 32 / 256 threads / four CTAs, 64 x 32 / 256 threads, 32 x 64 and
+// 64 x 32 / 512 threads with 4-cell batches: fastest at T = 4 and T = 6 on
+// 2048 x 512 and 4096 x 1024); shape 1 is the 32 x 32 tile with four CTAs per SM.
 template <int VAR, int SHAPE> static int aa_dispatch_shape(const AaParams &p, int T, cudaStream_t s)
 {
-    constexpr int SX = SHAPE == 0 ? 64 : 32, SY = 32, NT = SHAPE == 0 ? 256 : 256, NB = SHAPE == 0 ? 4 : 2;
-    constexpr int MB = SHAPE == 0 ? 2 : 4; // 4 CTAs (64 registers) per SM measured faster than 3
+    constexpr int SX = SHAPE == 2 ? 64 : 32, SY = 32, NT = SHAPE == 2 ? 512 : 256, NB = 2;
+    constexpr int MB = SHAPE == 2 ? 2 : 4;
     constexpr int MODE = VAR == VARIANT_SMEMAA ? MODE_PRE_SMEMAA : MODE_PRE_POLICY;
     bool done = false;
     int rc = LBM_OK;
@@ -104,10 +106,10 @@ template <int VAR> static int aa_dispatch(const AaParams &p, int T, cudaStream_t
 {
     static int shape = -1;
     if (shape < 0) {
-        const char *e = getenv("LBM_AA_SHAPE"); // tuning override for experiments
-        shape = (e && atoi(e) == 0) ? 0 : 1;
+        const char *e = getenv("LBM_AA_SHAPE"); // tuning override for experiments: 1 = 32 x 32 tiles
+        shape = (e && atoi(e) == 1) ? 1 : 2;
     }
-    return shape == 0 ? aa_dispatch_shape<VAR, 0>(p, T, s) : aa_dispatch_shape<VAR, 1>(p, T, s);
+    return shape == 1 ? aa_dispatch_shape<VAR, 1>(p, T, s) : aa_dispatch_shape<VAR, 2>(p, T, s);
 }
 
 // Split launch for T = 2, 4, 6 on TMA-aligned buffers: the reference's AA slot
@@ -150,9 +152,13 @@ template <class Cfg, int MODE>
 static int aa_split(AaParams p, int T, cudaStream_t s, bool &done)
 {
     done = false;
-    if (const char *e = getenv("LBM_AA_SPLIT"))
+    // LBM_AA_SPLIT=0: never split; =2: split at any size (tuning experiments)
+    int force = 0;
+    if (const char *e = getenv("LBM_AA_SPLIT")) {
         if (atoi(e) == 0)
             return LBM_OK;
+        force = atoi(e) == 2;
+    }
     constexpr int CX = Cfg::CX, CY = Cfg::CY;
     const int W = p.W, H = p.H;
     const bool al = aligned16(p.f_in) && aligned16(p.f_out) && aligned16(p.mask) && W % 16 == 0 &&
@@ -163,7 +169,7 @@ static int aa_split(AaParams p, int T, cudaStream_t s, bool &done)
     // the split pays on domains larger than the L2 cache (measured: 1.3x the tile
     // kernel at 4096 x 1024, 0.8x at 2048 x 512 where the interior is too small to
     // fill the GPU with full-length work items)
-    if (!al || etx1 - etx0 < 2 || ety1 - ety0 < 1 || (CX & 1) || (long long)W * H < (4ll << 20))
+    if (!al || etx1 - etx0 < 2 || ety1 - ety0 < 1 || (CX & 1) || (!force && (long long)W * H < (4ll << 20)))
         return LBM_OK;
     // edge band: the tile kernel on the tiles outside the interior block
     p.edge_only = 1;
