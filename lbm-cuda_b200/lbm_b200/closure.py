@@ -224,9 +224,11 @@ def smagorinsky_nu(x, cs: float, tau0: float):
 # ---------------------------------------------------------------------------
 # the decaying-turbulence judge and the a-posteriori comparison
 # ---------------------------------------------------------------------------
-def _run_periodic(N, f0, mask, n_steps, snap_every, T=2, **params):
+def _run_periodic(N, f0, mask, n_steps, snap_every, T=2, on_snap=None, timing=None, **params):
     """Periodic N x N run through the slab layer (one rank, so that the register
-    wavefront kernel applies); returns u, v, rho every snap_every steps (incl. 0)."""
+    wavefront kernel applies); returns u, v, rho every snap_every steps (incl. 0),
+    or on_snap(u, v, rho) of each when given.  `timing`, a dict, receives the
+    device milliseconds of the time stepping (CUDA events around the runs)."""
     import torch
 
     from . import solver as SV
@@ -251,48 +253,67 @@ def _run_periodic(N, f0, mask, n_steps, snap_every, T=2, **params):
         r = f.sum(0)
         return ((f * cx).sum(0) / r).cpu().numpy(), ((f * cy).sum(0) / r).cpu().numpy(), r.cpu().numpy()
 
-    snaps.append(macros())
-    done = 0
+    keep = on_snap if on_snap is not None else (lambda *a: a)
+    snaps.append(keep(*macros()))
+    done, ms = 0, 0.0
     while done < n_steps:
         k = min(snap_every, n_steps - done)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
         S.run(k)
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
         done += k
-        snaps.append(macros())
+        snaps.append(keep(*macros()))
+    if timing is not None:
+        timing["ms"] = ms
+        timing["cells"] = N * N
+        timing["steps"] = n_steps
     return snaps
 
 
 def filtered_judge(N: int, factor: int = 4, k0: float = 4.0, u_rms: float = 0.1 * 0.5773502691896258,
-                   nu: float = 5e-4, n_steps: int = 600, snap_every: int = 100, seed: int = 0, fine_cs: float = 0.0):
+                   nu: float = 5e-4, n_steps: int = 600, snap_every: int = 100, seed: int = 0, fine_cs: float = 0.0,
+                   balanced: bool = False, rates=(1.1, 1.1, 1.1)):
     """Runs the factor-finer decaying turbulence (MRT, nu_fine = factor nu,
     factor n_steps steps) and returns its snapshots filtered onto N x N, the
-    coarse initial state, and a-priori training data (features, nu*) per snapshot."""
+    coarse initial state, and a-priori training data (features, nu*) per snapshot.
+    balanced: start from the pressure-balanced density (spectral.balanced_density)
+    on both grids instead of rho = 1.  rates: the MRT ghost-moment rates
+    (s_e, s_eps, s_q) of both grids' solvers."""
     import torch
 
     from . import solver as SV
     from .init import equilibrium
-    from .spectral import box_filter, random_phase_velocity
+    from .spectral import balanced_density, box_filter, random_phase_velocity
 
     Nf = N * factor
     ux, uy = random_phase_velocity(Nf, k0, u_rms, seed)
-    f0 = equilibrium(np.ones((Nf, Nf)), ux, uy, dtype=np.float32)
+    rho_f = balanced_density(ux, uy) if balanced else np.ones((Nf, Nf))
+    f0 = equilibrium(rho_f, ux, uy, dtype=np.float32)
     nu_f = factor * nu
     tau_f = 3.0 * nu_f + 0.5
     mask = torch.zeros((Nf, Nf), dtype=torch.uint8)
     closure = dict(closure=SV.CLOSURE_SMAG, cs_smag=fine_cs) if fine_cs > 0 else dict(closure=SV.CLOSURE_NONE)
-    snaps = _run_periodic(Nf, f0, mask, factor * n_steps, factor * snap_every, s_nu=1.0 / tau_f, ref_clamps=0,
-                          **closure)
     tau0 = 3.0 * nu + 0.5
-    judge, data = [], []
-    for (u, v, r) in snaps:
-        judge.append((box_filter(u, factor), box_filter(v, factor)))
+
+    def reduce(u, v, r):  # filter each fine snapshot at once (a 4096^2 one is 400 MB)
         if not (np.isfinite(u).all() and np.isfinite(v).all()):
             raise FloatingPointError("the high-resolution run became unstable; raise its viscosity or Smagorinsky "
                                      "constant")
-        data.append(targets_and_features(u, v, r, factor, tau0=tau0, s_e=1.1))
+        return (box_filter(u, factor), box_filter(v, factor)), targets_and_features(u, v, r, factor, tau0=tau0,
+                                                                                      s_e=rates[0])
+
+    timing = {}
+    red = _run_periodic(Nf, f0, mask, factor * n_steps, factor * snap_every, on_snap=reduce, timing=timing,
+                        s_nu=1.0 / tau_f, ref_clamps=0, s_e=rates[0], s_eps=rates[1], s_q=rates[2], **closure)
+    judge = [j for j, _ in red]
+    data = [d for _, d in red]
     ub, vb = box_filter(ux, factor), box_filter(uy, factor)
-    fc = equilibrium(np.ones((N, N)), ub, vb, dtype=np.float32)
+    fc = equilibrium(box_filter(rho_f, factor), ub, vb, dtype=np.float32)
     return {"judge": judge, "data": data, "coarse_f0": fc, "tau0": tau0, "N": N, "factor": factor,
-            "snap_every": snap_every, "n_steps": n_steps}
+            "snap_every": snap_every, "n_steps": n_steps, "fine_timing": timing, "rates": tuple(rates)}
 
 
 def velocity_error(snaps, judge):
@@ -305,8 +326,10 @@ def velocity_error(snaps, judge):
     return out
 
 
-def spectrum_error(snaps, judge):
-    """L2 distance of log10 energy spectra (shells 1 .. N/2) to the judge's, per snapshot."""
+def spectrum_error(snaps, judge, rel_floor: float | None = None):
+    """L2 distance of log10 energy spectra (shells 1 .. N/2) to the judge's, per
+    snapshot; with rel_floor, only over the shells where the judge's energy is at
+    least rel_floor times its largest shell (leaving out shells at round-off level)."""
     from .spectral import energy_spectrum
 
     out = []
@@ -314,21 +337,28 @@ def spectrum_error(snaps, judge):
         _, e = energy_spectrum(u, v)
         _, ej = energy_spectrum(uj, vj)
         a, b = np.log10(np.maximum(e[1:], 1e-30)), np.log10(np.maximum(ej[1:], 1e-30))
+        if rel_floor is not None:
+            keep = ej[1:] >= rel_floor * ej[1:].max()
+            a, b = a[keep], b[keep]
         out.append(float(np.sqrt(np.mean((a - b) ** 2))))
     return out
 
 
-def compare_closures(J, net: "Mlp", cs: float = 0.1, storage: int = 0, T: int = 2):
+def compare_closures(J, net: "Mlp", cs: float = 0.1, storage: int = 0, T: int = 2, timings=None,
+                     spectrum_floor: float | None = None):
     """Coarse runs from the filtered initial state with no closure, Smagorinsky
     (Cs) and the network; relative L2 velocity error and log-spectrum error
-    against the judge per snapshot, for each: {name: (l2, spectrum)}."""
+    against the judge per snapshot, for each: {name: (l2, spectrum)}.
+    `timings`, a dict, receives each run's device time ({name: timing});
+    spectrum_floor is spectrum_error's rel_floor."""
     import torch
 
     from . import solver as SV
 
     N = J["N"]
     mask = torch.zeros((N, N), dtype=torch.uint8)
-    base = dict(s_nu=1.0 / J["tau0"], ref_clamps=0, storage=storage)
+    se, seps, sq = J.get("rates", (1.1, 1.1, 1.1))
+    base = dict(s_nu=1.0 / J["tau0"], ref_clamps=0, storage=storage, s_e=se, s_eps=seps, s_q=sq)
     res = {}
     for name, extra in (("none", dict(closure=SV.CLOSURE_NONE)), ("smagorinsky", dict(closure=SV.CLOSURE_SMAG,
                                                                                            cs_smag=cs)),
@@ -337,8 +367,11 @@ def compare_closures(J, net: "Mlp", cs: float = 0.1, storage: int = 0, T: int = 
         if storage != SV.STORE_F32:
             f0 = f0 - np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, np.float32)[:, None, None]
             f0 = torch.from_numpy(f0).to(torch.float16 if storage == SV.STORE_F16DEV else torch.bfloat16)
-        snaps = _run_periodic(N, f0, mask, J["n_steps"], J["snap_every"], T=T, **base, **extra)
-        res[name] = (velocity_error(snaps, J["judge"]), spectrum_error(snaps, J["judge"]))
+        tm = {}
+        snaps = _run_periodic(N, f0, mask, J["n_steps"], J["snap_every"], T=T, timing=tm, **base, **extra)
+        res[name] = (velocity_error(snaps, J["judge"]), spectrum_error(snaps, J["judge"], spectrum_floor))
+        if timings is not None:
+            timings[name] = tm
     return res
 
 

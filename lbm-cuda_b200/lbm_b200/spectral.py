@@ -54,6 +54,28 @@ def random_phase_velocity(N: int, k0: float = 8.0, u_rms: float = 0.1 * CS, seed
     return ux * s, uy * s
 
 
+def balanced_density(ux, uy, rho0: float = 1.0):
+    """Density whose pressure balances an incompressible periodic velocity field:
+    the pressure Poisson equation lap p = -d_i d_j (u_i u_j), solved spectrally
+    (p_hat = -k_i k_j (u_i u_j)_hat / |k|^2, zero mean), and rho = rho0 (1 + p / c_s^2)
+    with c_s^2 = 1/3.  Starting a decaying-turbulence run from this density
+    instead of a uniform one removes the acoustic pulse of the vortex cores'
+    missing pressure dip, which on large grids steepens into grid-scale waves."""
+    ux = np.asarray(ux, dtype=np.float64)
+    uy = np.asarray(uy, dtype=np.float64)
+    N = ux.shape[0]
+    kx, ky = _wavenumbers(N)
+    kx = kx * (2.0 * np.pi / N)
+    ky = ky * (2.0 * np.pi / N)
+    k2 = kx * kx + ky * ky
+    k2[0, 0] = 1.0
+    rhs = (kx * kx * np.fft.fft2(ux * ux) + 2.0 * kx * ky * np.fft.fft2(ux * uy) + ky * ky * np.fft.fft2(uy * uy))
+    ph = -rhs / k2
+    ph[0, 0] = 0.0
+    p = np.real(np.fft.ifft2(ph))
+    return rho0 * (1.0 + 3.0 * p)
+
+
 def spectral_divergence(ux, uy) -> float:
     """max |k . u_hat| / max |k| |u_hat| (0 for a divergence-free periodic field)."""
     N = ux.shape[0]
@@ -100,9 +122,12 @@ def box_filter(a, f: int):
     return a.reshape(a.shape[:-2] + (N0 // f, f, N1 // f, f)).mean(axis=(-3, -1))
 
 
-def turbulence_state(N: int, k0: float = 8.0, u_rms: float = 0.1 * CS, seed: int = 0, dtype=np.float32):
-    """Equilibrium populations (9, N, N) of rho = 1 and the random-phase velocity."""
+def turbulence_state(N: int, k0: float = 8.0, u_rms: float = 0.1 * CS, seed: int = 0, dtype=np.float32,
+                     balanced: bool = False):
+    """Equilibrium populations (9, N, N) of the random-phase velocity and rho = 1
+    (or, balanced, the density of :func:`balanced_density`)."""
     from .init import equilibrium
 
     ux, uy = random_phase_velocity(N, k0, u_rms, seed)
-    return equilibrium(np.ones((N, N)), ux, uy, dtype=dtype)
+    rho = balanced_density(ux, uy) if balanced else np.ones((N, N))
+    return equilibrium(rho, ux, uy, dtype=dtype)

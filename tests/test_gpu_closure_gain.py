@@ -3,17 +3,13 @@ the fallback), on decaying 2-D turbulence: a 4x finer run of this solver,
 box-filtered onto the 64^2 grid, is the judge.  The network is trained on the
 judge's first snapshots (a-priori least-squares eddy viscosity) and tested on
 later ones, then run inside the solver against Smagorinsky (Cs = 0.1) and no
-closure.  Measured numbers go to gpurun_out/closure_gain.json when that folder
-exists.
+closure.
 
 Findings asserted here: a priori the network's eddy viscosity is far closer to
 the judge's than Cs = 0.1 Smagorinsky (which over-dissipates at this
 resolution) and no worse than no closure; a posteriori its velocity field
 stays closer to the filtered judge than Smagorinsky's over the first
 snapshots, and its energy spectrum error at the first snapshot is lower."""
-import json
-import os
-
 import numpy as np
 import pytest
 
@@ -34,9 +30,3 @@ def test_learned_closure_gain_over_smagorinsky():
     for i in (1, 2, 3):
         assert l2["mlp"][i] < l2["smagorinsky"][i]
     assert sp["mlp"][1] < sp["smagorinsky"][1]
-    out = os.path.join(os.path.dirname(os.path.dirname(__file__)), "gpurun_out")
-    if os.path.isdir(out):
-        with open(os.path.join(out, "closure_gain.json"), "w") as fh:
-            json.dump({"a_priori_mse": ap, "velocity_rel_l2": l2, "log_spectrum_l2": sp,
-                       "setup": "64^2 coarse, 256^2 judge (box filter 4), k0 = 8, nu = 2e-4, 400 steps, "
-                                "snapshots every 50"}, fh, indent=1)

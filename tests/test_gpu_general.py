@@ -5,7 +5,6 @@ Tolerances: FP32 storage, relative L2 <= 1e-5 on the populations and on u, v,
 rho of the last step (helpers.REL_TOL).  16-bit deviation storage is compared
 with the FP64 oracle and its error is printed and bounded (see
 test_storage_formats_error)."""
-import json
 import os
 
 import numpy as np
@@ -192,10 +191,6 @@ def test_storage_formats_error():
             errs[f"storage{storage}_T{T}"] = err
             assert err < bound, (storage, T, err)
     print("velocity rel L2 vs FP64 oracle after 200 steps:", errs)
-    out = os.path.join(os.path.dirname(os.path.dirname(__file__)), "gpurun_out")
-    if os.path.isdir(out):
-        with open(os.path.join(out, "storage_errors.json"), "w") as fh:
-            json.dump(errs, fh, indent=1)
 
 
 @pytest.mark.parametrize("storage", [SV.STORE_F32, SV.STORE_F16DEV])

@@ -68,3 +68,23 @@ def test_decaying_turbulence_on_gpu():
     k, Ed = SP.energy_spectrum(mac[0], mac[1])
     _, Eh = SP.energy_spectrum(host(mac[0]).astype(np.float64), host(mac[1]).astype(np.float64))
     assert np.allclose(Ed, Eh, rtol=1e-9, atol=1e-16)
+
+
+def test_balanced_density_solves_the_pressure_poisson_equation():
+    """rho = 1 + 3 p with lap p = -d_i d_j (u_i u_j) (spectral, periodic)."""
+    N = 128  # k0 = 4: the products u_i u_j stay well below the Nyquist wavenumber
+    ux, uy = SP.random_phase_velocity(N, 4.0, 0.1 * SP.CS, 5)
+    rho = SP.balanced_density(ux, uy)
+    p = (rho - 1.0) / 3.0
+    k = np.fft.fftfreq(N, d=1.0 / N) * 2.0 * np.pi / N
+    ky, kx = np.meshgrid(k, k, indexing="ij")
+    F = np.fft.fft2
+    lap_p = -(kx * kx + ky * ky) * F(p)
+    rhs = (kx * kx * F(ux * ux) + 2.0 * kx * ky * F(ux * uy) + ky * ky * F(uy * uy))
+    inner = np.ones((N, N), bool)
+    inner[N // 2, :] = inner[:, N // 2] = False  # the Nyquist row and column are not Hermitian for k_x k_y
+    assert np.abs((lap_p - rhs)[inner]).max() < 1e-10 * np.abs(rhs).max()  # -k^2 p_hat = k_i k_j (u_i u_j)_hat
+    assert abs(p.mean()) < 1e-15
+    # vortex cores (high speed) sit at low pressure
+    sp = np.hypot(ux, uy)
+    assert np.corrcoef(sp.ravel(), p.ravel())[0, 1] < 0
