@@ -24,6 +24,8 @@ reference does (lbm_mine2.py:106).
 
 --workload batch times 256 independent channel domains of uneven size in one
 persistent launch per T steps (FP16 storage) against one launch per domain.
+--workload c2 runs the cylinder workload for 50 000 steps with drag and lift
+sampled every 100 steps (mean drag coefficient, RMS lift, Strouhal number).
 --workload c3 runs the 8192 x 2048 cylinder (D = 256, Re = 20 000) in FP32, FP16
 and BF16 deviation storage to 1k / 10k / 50k steps and reports the 16-bit runs'
 velocity error against the FP32 run, and each format's MLUPS at that size.
@@ -193,7 +195,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32",
                     help="population storage of the cylinder workload (16-bit: deviations f - w)")
-    ap.add_argument("--workload", choices=["cylinder", "batch", "dropins", "c3", "c4"], default="cylinder")
+    ap.add_argument("--workload", choices=["cylinder", "batch", "dropins", "c2", "c3", "c4"], default="cylinder")
+    ap.add_argument("--c2-steps", type=int, default=50000, help="c2: physical steps")
+    ap.add_argument("--c2-out", default=None, help="c2: CSV file for the drag / lift series")
     ap.add_argument("--c4-n", type=int, default=1024, help="c4: coarse grid (the judge is 4x finer)")
     ap.add_argument("--c4-steps", type=int, default=20000, help="c4: coarse steps")
     ap.add_argument("--c4-epochs", type=int, default=30, help="c4: training epochs")
@@ -239,9 +243,11 @@ def main():
     from lbm_b200 import solver as SV
     from lbm_b200.solver import Solver
 
-    if args.workload in ("batch", "dropins", "c3", "c4"):
+    if args.workload in ("batch", "dropins", "c2", "c3", "c4"):
         if args.workload == "batch":
             line = run_batch(args, torch, rank, world, barrier, max_over_ranks)
+        elif args.workload == "c2":
+            line = run_c2(args, torch)
         elif args.workload == "c3":
             line = run_c3(args, torch)
         elif args.workload == "c4":
@@ -479,6 +485,68 @@ def run_batch(args, torch, rank, world, barrier, max_over_ranks):
         "gpu_launches": args.steps * ((steps_per + T - 1) // T),
         "clocks": clk.summary(),
     }
+
+
+def run_c2(args, torch):
+    """The cylinder workload (4096 x 1024, D = 128, Re = 10 000, MRT + Smagorinsky
+    Cs = 0.1, Zou-He u = 0.05 with the ramp) run for --c2-steps steps at T = 2,
+    with drag and lift (lbm_forces_fp64, momentum exchange on the cylinder)
+    sampled every 100 steps into device memory.  Reports the drag and lift
+    coefficients C = F / (0.5 rho u^2 D) over the second half of the run, the
+    Strouhal number f D / u of the lift's dominant frequency there, and the
+    MLUPS of the whole run including the force reductions; --c2-out writes the
+    series (step, Fx, Fy, Cd, Cl) as CSV."""
+    from lbm_b200 import solver as SV
+
+    mask_np, f0_np = workload()
+    mask = torch.from_numpy(mask_np).cuda()
+    S = SV.Solver(W, H, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU)
+    a = torch.from_numpy(f0_np).cuda()
+    b = a.clone()
+    every, T = 100, 2
+    n = max(2, args.c2_steps // every)
+    series = torch.zeros((n, 2), dtype=torch.float64, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(n):
+        if S.run(a, b, mask, every, T):
+            a, b = b, a
+        S.forces(a, mask, out=series[i])
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    F = series.cpu().numpy()
+    D = float(CYL[2])
+    q = 0.5 * 1.0 * U_IN * U_IN * D
+    cd, cl = F[:, 0] / q, F[:, 1] / q
+    steps = (np.arange(n) + 1) * every
+    half = slice(n // 2, n)
+    x = cl[half] - cl[half].mean()
+    spec = np.abs(np.fft.rfft(x * np.hanning(x.size))) ** 2
+    freq = np.fft.rfftfreq(x.size, d=float(every))  # per step
+    k = 1 + int(np.argmax(spec[1:]))
+    st = float(freq[k] * D / U_IN)
+    # peak refined by a parabola through the log power of the three bins around it
+    la, lb, lc = np.log(spec[k - 1] + 1e-300), np.log(spec[k] + 1e-300), np.log(spec[min(k + 1, spec.size - 1)] + 1e-300)
+    den = la - 2.0 * lb + lc
+    st_fit = float((k + (0.5 * (la - lc) / den if den != 0 else 0.0)) * freq[1] * D / U_IN)
+    if args.c2_out:
+        np.savetxt(args.c2_out, np.column_stack([steps, F[:, 0], F[:, 1], cd, cl]), delimiter=",",
+                   header="step,Fx,Fy,Cd,Cl", comments="")
+    return {"metric": "MLUPS", "value": round(W * H * n * every / (ms * 1e3), 1), "unit": "MLUPS", "n_gpus": 1,
+            "steps": n * every, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"cylinder channel {W}x{H} D2Q9 MRT+Smagorinsky Cs={CS}, Zou-He u={U_IN} "
+                                   f"(ramp), D={CYL[2]} at ({CYL[0]},{CYL[1]}), Re={U_IN * D / NU:.0f}, T={T}, "
+                                   f"forces every {every} steps"},
+            "drag_lift": {"cd_mean_second_half": round(float(cd[half].mean()), 4),
+                          "cd_std_second_half": round(float(cd[half].std()), 4),
+                          "cl_rms_second_half": round(float(np.sqrt(np.mean(x ** 2))), 4),
+                          "strouhal_second_half": round(st, 4),
+                          "strouhal_resolution": round(float(freq[1] * D / U_IN), 4),
+                          "strouhal_refined_second_half": round(st_fit, 4),
+                          "finite": bool(np.isfinite(F).all()),
+                          "cd_last": round(float(cd[-1]), 4), "cl_last": round(float(cl[-1]), 4)}}
 
 
 def run_c3(args, torch):
