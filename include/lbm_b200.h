@@ -215,8 +215,8 @@ int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk)
 /* Read (and optionally clear) the device error word of the current device:
  * bit 0 = a bounded device-side wait gave up.  Synchronises the device. */
 /* ------------------------------------------------------------------------
- * Learned closure (no reference counterpart): a 5 -> 32 -> 32 -> 1 MLP (SiLU,
- * SiLU, softplus) maps per-cell features to an eddy viscosity nu_t >= 0; the
+ * Learned closure (no reference counterpart): a 5 -> 32 -> 32 -> 1 MLP (ReLU,
+ * ReLU, softplus) maps per-cell features to an eddy viscosity nu_t >= 0; the
  * collision then relaxes the stress moments with 1 / (1/s_nu + 3 nu_t) in
  * place of the Smagorinsky rate.  Features of a cell, from its pre-collision
  * populations: the non-equilibrium stress moments n7 = P_xx - P_yy - rho (u^2 -

@@ -1,4 +1,4 @@
-// Learned closure, inference side: the 5 -> 32 -> 32 -> 1 MLP (SiLU, SiLU,
+// Learned closure, inference side: the 5 -> 32 -> 32 -> 1 MLP (ReLU, ReLU,
 // softplus) evaluated by one warp for 64 cells (two per lane) on the tensor
 // cores with mma.sync.m16n8k16 (BF16 inputs, FP32 accumulation).
 //
@@ -7,16 +7,19 @@
 //               column 5 holds b1 (the staged features carry a constant 1
 //               there), columns 6..15 zero;
 //   w2[32][32], w3[8][32] (row 0 = w3, rows 1..7 zero), b2[32], b3, out_scale;
-//   w1, b1, w2 and b2 are stored at half scale (see silu_half_bf16x2).
+//   all unscaled (BF16 weights; b2, b3 and out_scale FP32).
 //
 // Per warp: the 64 feature rows are staged as BF16 in 1 KB of shared memory
 // (row c = cell c = 2 lane + n, 8 values: 5 features, 1, 0, 0) and read as A
 // fragments; a layer's accumulators become the next layer's A fragments in
 // registers (the m16n8k16 accumulator layout of two adjacent 8-column tiles is
-// the A layout of one 16-wide k tile).  SiLU runs on BF16 pairs:
-// silu(a) = a/2 (1 + tanh(a/2)) with tanh.approx.bf16x2, one transcendental per
-// two activations (on the half-scale accumulators).  The output z of a cell is
-// nu_t = out_scale softplus(z).
+// the A layout of one 16-wide k tile).  The activation is ReLU, applied by the
+// FP32 -> BF16x2 conversion that packs the accumulators anyway
+// (cvt.rn.relu.bf16x2.f32), so it costs no instruction; the accumulators start
+// from the bias (or zero) passed as the MMA's C operand.  (A SiLU via
+// tanh.approx.bf16x2 costs a transcendental-unit instruction per pair, which
+// runs at 8 per clock per SM against about 60 for the conversion, and bounded
+// the kernel.)  The output z of a cell is nu_t = out_scale softplus(z).
 #pragma once
 
 #include "collide.cuh"
@@ -72,12 +75,14 @@ __device__ __forceinline__ void mlp_load_frag(const MlpPacked *W, MlpFrag &F, in
     F.out_scale = W->out_scale;
 }
 
-__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+// d = a b + c (m16n8k16, BF16 inputs, FP32 accumulators)
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1, float c0,
+                                         float c1, float c2, float c3)
 {
-    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
-                 "{%8, %9}, {%0, %1, %2, %3};"
-                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+        "{%8, %9}, {%10, %11, %12, %13};"
+        : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1), "f"(c0), "f"(c1), "f"(c2), "f"(c3));
 }
 
 // BF16 pair {lo, hi} (lo in the low half).
@@ -88,14 +93,12 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi)
     return d;
 }
 
-// silu(a) of a BF16 pair given h = a/2 (the packed layers are at half scale):
-// a sigmoid(a) = a/2 (1 + tanh(a/2)) = h + h tanh(h).
-__device__ __forceinline__ uint32_t silu_half_bf16x2(uint32_t h)
+// BF16 pair {relu(lo), relu(hi)}: the activation and the packing in one conversion.
+__device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi)
 {
-    uint32_t th, r;
-    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(th) : "r"(h));
-    asm("fma.rn.bf16x2 %0, %1, %2, %3;" : "=r"(r) : "r"(h), "r"(th), "r"(h));
-    return r;
+    uint32_t d;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+    return d;
 }
 
 // Eddy viscosity of the lane's two cells from their features x[n][5].  Warp-
@@ -127,42 +130,35 @@ __device__ __forceinline__ void mlp_nu_t(const MlpFrag &F, const float (&x)[2][5
         a[3] = 0u;
         float h1[4][4];
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-            h1[nt][0] = h1[nt][1] = h1[nt][2] = h1[nt][3] = 0.0f;
-            mma_bf16(h1[nt], a, F.b1[nt][0], F.b1[nt][1]);
-        }
-        // SiLU -> layer-2 A fragments (k tile kt = hidden 16 kt .. 16 kt + 15)
+        for (int nt = 0; nt < 4; ++nt)
+            mma_bf16(h1[nt], a, F.b1[nt][0], F.b1[nt][1], 0.0f, 0.0f, 0.0f, 0.0f);
+        // ReLU -> layer-2 A fragments (k tile kt = hidden 16 kt .. 16 kt + 15)
         uint32_t a2[2][4];
 #pragma unroll
         for (int kt = 0; kt < 2; ++kt) {
-            a2[kt][0] = silu_half_bf16x2(pack_bf16x2(h1[2 * kt][0], h1[2 * kt][1]));
-            a2[kt][1] = silu_half_bf16x2(pack_bf16x2(h1[2 * kt][2], h1[2 * kt][3]));
-            a2[kt][2] = silu_half_bf16x2(pack_bf16x2(h1[2 * kt + 1][0], h1[2 * kt + 1][1]));
-            a2[kt][3] = silu_half_bf16x2(pack_bf16x2(h1[2 * kt + 1][2], h1[2 * kt + 1][3]));
+            a2[kt][0] = relu_bf16x2(h1[2 * kt][0], h1[2 * kt][1]);
+            a2[kt][1] = relu_bf16x2(h1[2 * kt][2], h1[2 * kt][3]);
+            a2[kt][2] = relu_bf16x2(h1[2 * kt + 1][0], h1[2 * kt + 1][1]);
+            a2[kt][3] = relu_bf16x2(h1[2 * kt + 1][2], h1[2 * kt + 1][3]);
         }
         float h2[4][4];
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
-            h2[nt][0] = F.c2[nt][0];
-            h2[nt][1] = F.c2[nt][1];
-            h2[nt][2] = F.c2[nt][0];
-            h2[nt][3] = F.c2[nt][1];
-#pragma unroll
-            for (int kt = 0; kt < 2; ++kt)
-                mma_bf16(h2[nt], a2[kt], F.b2[nt][kt][0], F.b2[nt][kt][1]);
+            float t2[4];
+            mma_bf16(t2, a2[0], F.b2[nt][0][0], F.b2[nt][0][1], F.c2[nt][0], F.c2[nt][1], F.c2[nt][0], F.c2[nt][1]);
+            mma_bf16(h2[nt], a2[1], F.b2[nt][1][0], F.b2[nt][1][1], t2[0], t2[1], t2[2], t2[3]);
         }
         uint32_t a3[2][4];
 #pragma unroll
         for (int kt = 0; kt < 2; ++kt) {
-            a3[kt][0] = silu_half_bf16x2(pack_bf16x2(h2[2 * kt][0], h2[2 * kt][1]));
-            a3[kt][1] = silu_half_bf16x2(pack_bf16x2(h2[2 * kt][2], h2[2 * kt][3]));
-            a3[kt][2] = silu_half_bf16x2(pack_bf16x2(h2[2 * kt + 1][0], h2[2 * kt + 1][1]));
-            a3[kt][3] = silu_half_bf16x2(pack_bf16x2(h2[2 * kt + 1][2], h2[2 * kt + 1][3]));
+            a3[kt][0] = relu_bf16x2(h2[2 * kt][0], h2[2 * kt][1]);
+            a3[kt][1] = relu_bf16x2(h2[2 * kt][2], h2[2 * kt][3]);
+            a3[kt][2] = relu_bf16x2(h2[2 * kt + 1][0], h2[2 * kt + 1][1]);
+            a3[kt][3] = relu_bf16x2(h2[2 * kt + 1][2], h2[2 * kt + 1][3]);
         }
-        float z[4] = {F.b3v, 0.0f, F.b3v, 0.0f};
-#pragma unroll
-        for (int kt = 0; kt < 2; ++kt)
-            mma_bf16(z, a3[kt], F.b3[kt][0], F.b3[kt][1]);
+        float z0[4], z[4];
+        mma_bf16(z0, a3[0], F.b3[0][0], F.b3[0][1], F.b3v, 0.0f, F.b3v, 0.0f);
+        mma_bf16(z, a3[1], F.b3[1][0], F.b3[1][1], z0[0], z0[1], z0[2], z0[3]);
         if (t == 0) { // column 0 of rows g and g + 8
             zbuf[r0] = z[0];
             zbuf[r0 + 8] = z[2];

@@ -1,5 +1,5 @@
-// Training kernels of the learned closure: a 5 -> 32 -> 32 -> 1 MLP (SiLU, SiLU,
-// softplus) mapping per-cell features to an eddy viscosity.  FP32 master weights,
+// Training kernels of the learned closure: a 5 -> 32 -> 32 -> 1 MLP (ReLU,
+// ReLU, softplus) mapping per-cell features to an eddy viscosity.  FP32 master weights,
 // one thread per sample; the weight gradient is reduced deterministically
 // (per-block partial sums in a fixed order, then a fixed-order sum over blocks).
 //
@@ -22,6 +22,15 @@ __device__ __forceinline__ float sigm(float x)
 {
     return 1.0f / (1.0f + expf(-x));
 }
+// ReLU and its derivative (1 for a > 0, else 0)
+__device__ __forceinline__ float relu(float a)
+{
+    return fmaxf(a, 0.0f);
+}
+__device__ __forceinline__ float relu_grad(float a)
+{
+    return a > 0.0f ? 1.0f : 0.0f;
+}
 __device__ __forceinline__ float softplus(float x)
 {
     return x > 20.0f ? x : log1pf(expf(x));
@@ -38,7 +47,7 @@ __device__ __forceinline__ float forward1(const float *P, const float *x, float 
         for (int k = 0; k < NI; ++k)
             s = fmaf(P[OW1 + i * NI + k], x[k], s);
         a1[i] = s;
-        h1[i] = s * sigm(s);
+        h1[i] = relu(s);
     }
 #pragma unroll
     for (int i = 0; i < NH; ++i) {
@@ -47,7 +56,7 @@ __device__ __forceinline__ float forward1(const float *P, const float *x, float 
         for (int k = 0; k < NH; ++k)
             s = fmaf(P[OW2 + i * NH + k], h1[k], s);
         a2[i] = s;
-        h2[i] = s * sigm(s);
+        h2[i] = relu(s);
     }
     float s = P[OB3];
 #pragma unroll
@@ -106,22 +115,19 @@ __global__ void __launch_bounds__(BT) mlp_grad_kernel(const float *params, const
         for (int i = 0; i < NH; ++i)
             a1[i] = h1[i] = a2[i] = h2[i] = 0.0f;
     }
-    // dL/da2 = dz * w3 * silu'(a2), silu'(a) = s(a) (1 + a (1 - s(a)))
+    // dL/da2 = dz * w3 * relu'(a2)
     float d2[NH];
 #pragma unroll
-    for (int i = 0; i < NH; ++i) {
-        const float sg = sigm(a2[i]);
-        d2[i] = dz * P[OW3 + i] * sg * (1.0f + a2[i] * (1.0f - sg));
-    }
-    // dL/da1 = (W2^T d2) * silu'(a1)
+    for (int i = 0; i < NH; ++i)
+        d2[i] = dz * P[OW3 + i] * relu_grad(a2[i]);
+    // dL/da1 = (W2^T d2) * relu'(a1)
 #pragma unroll
     for (int k = 0; k < NH; ++k) {
         float g = 0.0f;
 #pragma unroll
         for (int i = 0; i < NH; ++i)
             g = fmaf(P[OW2 + i * NH + k], d2[i], g);
-        const float sg = sigm(a1[k]);
-        sd1[tid][k] = g * sg * (1.0f + a1[k] * (1.0f - sg));
+        sd1[tid][k] = g * relu_grad(a1[k]);
     }
 #pragma unroll
     for (int i = 0; i < NH; ++i) {
@@ -218,9 +224,8 @@ __global__ void mlp_adam_kernel(float *params, const float *grad, float *m, floa
     params[p] -= lr * (mm * c1) / (sqrtf(vv * c2) + eps);
 }
 
-// The hidden layers are stored at half scale (W1, b1, W2, b2 times 1/2): the
-// kernel's accumulators then hold a/2, and silu(a) = a/2 (1 + tanh(a/2)) is one
-// tanh and one fma on them.
+// Packing: W1 with in_scale folded in and b1 as column 5, W2, w3 in BF16; b2, b3
+// and out_scale in FP32.
 __global__ void mlp_pack_kernel(const float *P, const float *in_scale, float out_scale, MlpPacked *W)
 {
     const int tid = threadIdx.x;
@@ -231,14 +236,14 @@ __global__ void mlp_pack_kernel(const float *P, const float *in_scale, float out
             v = P[OW1 + n * NI + k] * in_scale[k];
         else if (k == NI)
             v = P[OB1 + n];
-        W->w1[n][k] = __float2bfloat16_rn(0.5f * v);
+        W->w1[n][k] = __float2bfloat16_rn(v);
     }
     for (int i = tid; i < 32 * 32; i += blockDim.x)
-        W->w2[i / 32][i % 32] = __float2bfloat16_rn(0.5f * P[OW2 + i]);
+        W->w2[i / 32][i % 32] = __float2bfloat16_rn(P[OW2 + i]);
     for (int i = tid; i < 8 * 32; i += blockDim.x)
         W->w3[i / 32][i % 32] = __float2bfloat16_rn(i < 32 ? P[OW3 + i] : 0.0f);
     for (int i = tid; i < 32; i += blockDim.x)
-        W->b2[i] = 0.5f * P[OB2 + i];
+        W->b2[i] = P[OB2 + i];
     if (tid == 0) {
         W->b3 = P[OB3];
         W->out_scale = out_scale;

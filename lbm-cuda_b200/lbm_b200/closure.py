@@ -3,7 +3,7 @@ solver, training on the GPU with the library's own forward / backward / Adam
 kernels (lbm_mlp_*), and packing for the collision kernel (LBM_CLOSURE_MLP).
 
 Model.  nu_t = out_scale * softplus(MLP(in_scale * x)), MLP 5 -> 32 -> 32 -> 1
-with SiLU; the collision relaxes the stress moments with 1 / (tau0 + 3 nu_t).
+with ReLU on both hidden layers; the collision relaxes the stress moments with 1 / (tau0 + 3 nu_t).
 The per-cell features x (what the kernel computes from the pre-collision
 populations) are the non-equilibrium stress moments n7 = Pi_xx - Pi_yy - rho
 (u^2 - v^2), n8 = Pi_xy - rho u v, the energy moment ne = e - rho (3 |u|^2 - 2),

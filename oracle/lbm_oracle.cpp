@@ -498,7 +498,7 @@ void visualize(const float *ux, const float *uy, uint8_t *img, const uint8_t *ma
 // BC codes: 0 wall, 1 periodic, 2 Zou-He, 3 Zou-He with ramp, 4 outflow.
 // ---------------------------------------------------------------------------
 // Learned closure (closure code 2): nu_t = out_scale softplus(MLP(in_scale x)),
-// MLP 5 -> 32 -> 32 -> 1 with SiLU, in double precision; x = (n7, n8, ne,
+// MLP 5 -> 32 -> 32 -> 1 with ReLU, in double precision; x = (n7, n8, ne,
 // |(n7, n8)|, rho - 1) of the pre-collision populations.  Parameters: W1[32][5],
 // b1[32], W2[32][32], b2[32], w3[32], b3 (set by orc_set_mlp).
 struct MlpParams {
@@ -508,6 +508,7 @@ struct MlpParams {
     bool set;
 };
 static MlpParams g_mlp = {{0}, {0}, 1.0, false};
+
 
 template <class S> inline S mlp_rate(const S *f, S r, S u, S v, S tau0)
 {
@@ -522,13 +523,13 @@ template <class S> inline S mlp_rate(const S *f, S r, S u, S v, S tau0)
         double a = P[160 + i];
         for (int k = 0; k < 5; ++k)
             a += P[i * 5 + k] * x[k] * g_mlp.in_scale[k];
-        h1[i] = a / (1.0 + std::exp(-a));
+        h1[i] = std::max(a, 0.0);
     }
     for (int i = 0; i < 32; ++i) {
         double a = P[192 + 1024 + i];
         for (int k = 0; k < 32; ++k)
             a += P[192 + i * 32 + k] * h1[k];
-        h2[i] = a / (1.0 + std::exp(-a));
+        h2[i] = std::max(a, 0.0);
     }
     double z = P[192 + 1024 + 32 + 32];
     for (int k = 0; k < 32; ++k)

@@ -1,6 +1,6 @@
 """Oracle of the learned-closure MLP (test infrastructure only): numpy FP64
-forward and backward of the 5 -> 32 -> 32 -> 1 network (SiLU, SiLU,
-softplus) with the parameter layout of lbm-cuda_b200/csrc/mlp_train.cu, and
+forward and backward of the 5 -> 32 -> 32 -> 1 network (ReLU on both
+hidden layers, softplus output) with the parameter layout of lbm-cuda_b200/csrc/mlp_train.cu, and
 the loss L = (1/n) sum_i w_i (y_i - t_i)^2 whose gradient lbm_mlp_grad
 returns.  No counterpart in the reference (the reference has no learned
 closure); the restatement follows the mathematics of the network."""
@@ -24,13 +24,21 @@ def _sig(a):
     return 1.0 / (1.0 + np.exp(-a))
 
 
+def relu(a):
+    return np.maximum(a, 0.0)
+
+
+def relu_grad(a):
+    return (a > 0.0).astype(np.float64)
+
+
 def forward(p, x):
     W1, b1, W2, b2, w3, b3 = unpack(p)
     x = np.asarray(x, np.float64)
     a1 = x @ W1.T + b1
-    h1 = a1 * _sig(a1)
+    h1 = relu(a1)
     a2 = h1 @ W2.T + b2
-    h2 = a2 * _sig(a2)
+    h2 = relu(a2)
     z = h2 @ w3 + b3
     y = np.where(z > 30, z, np.log1p(np.exp(np.minimum(z, 30))))
     return y, (x, a1, h1, a2, h2, z)
@@ -47,12 +55,10 @@ def loss_grad(p, x, t, w=None):
     g = np.zeros(NPARAM)
     g[OW3:OB3] = dz @ h2
     g[OB3] = dz.sum()
-    s2 = _sig(a2)
-    d2 = dz[:, None] * w3[None, :] * s2 * (1 + a2 * (1 - s2))
+    d2 = dz[:, None] * w3[None, :] * relu_grad(a2)
     g[OW2:OB2] = (d2.T @ h1).ravel()
     g[OB2:OW3] = d2.sum(0)
-    s1 = _sig(a1)
-    d1 = (d2 @ W2) * s1 * (1 + a1 * (1 - s1))
+    d1 = (d2 @ W2) * relu_grad(a1)
     g[OW1:OB1] = (d1.T @ x).ravel()
     g[OB1:OW2] = d1.sum(0)
     return loss, g
