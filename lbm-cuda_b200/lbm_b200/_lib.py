@@ -8,7 +8,9 @@ import subprocess
 import threading
 
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))  # lbm-cuda_b200/
-LIB_PATH = os.path.join(PKG_DIR, "liblbm_b200.so")
+# LBM_B200_LIB names another build of the library (for instance one compiled
+# with different tuning macros); the default is the in-tree build.
+LIB_PATH = os.environ.get("LBM_B200_LIB") or os.path.join(PKG_DIR, "liblbm_b200.so")
 
 _P, _I, _F, _D = C.c_void_p, C.c_int, C.c_float, C.c_double
 _IP = C.POINTER(C.c_int)
