@@ -149,6 +149,19 @@ int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *
 int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_steps, int T, float *ux, float *uy,
             float *rho, void *stream, int *result_in_b);
 
+/* n_steps steps in ONE state buffer (no counterpart in the reference, whose
+ * drivers ping-pong two buffers, lbm_mine2.py:77-80): half the state memory of
+ * lbm_run.  The AA access pattern: a pull-and-push step, then a step local to
+ * each cell, so that within each step every location is read and written by a
+ * single cell.  f holds the same post-collision state as lbm_run's buffers
+ * before and after; n_steps must be even (LBM_ERR_ARG otherwise), and the
+ * result equals lbm_run's for the same parameters (both of lbm_run's buffers
+ * initialised with the same state).  u, v, rho of the last step are written
+ * when the pointers are non-NULL.  The learned closure is not supported here
+ * (LBM_ERR_UNSUPPORTED). */
+int lbm_run_inplace(lbm_handle *h, void *f, const uint8_t *mask, int n_steps, float *ux, float *uy, float *rho,
+                    void *stream);
+
 /* Total mass and momentum sum_x sum_q f, c_x f, c_y f over cells with mask == 0,
  * accumulated in FP64 with a fixed-order two-pass reduction (deterministic).
  * d_out: 3 doubles of device memory. */

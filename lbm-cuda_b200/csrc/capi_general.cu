@@ -232,6 +232,16 @@ static int grid_for(long long n)
     return (int)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
+struct InplaceParams {
+    void *f;
+    const uint8_t *mask;
+    float *ux, *uy, *rho;
+    int W, H;
+    int bc_left, bc_right, bc_y;
+    Phys k;
+};
+int inplace_step(int variant, int storage, const InplaceParams &p, bool local, cudaStream_t s);
+
 } // namespace lbm
 
 using namespace lbm;
@@ -362,6 +372,43 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
     }
     if (result_in_b)
         *result_in_b = launches & 1;
+    return LBM_OK;
+}
+
+int lbm_run_inplace(lbm_handle *h, void *f, const uint8_t *mask, int n_steps, float *ux, float *uy, float *rho,
+                    void *stream)
+{
+    if (!h || !f || !mask || n_steps < 0 || (n_steps & 1))
+        return LBM_ERR_ARG;
+    if ((ux || uy || rho) && !(ux && uy && rho))
+        return LBM_ERR_ARG;
+    if (h->variant == VAR_MRT_MLP)
+        return LBM_ERR_UNSUPPORTED;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    InplaceParams ip;
+    memset(&ip, 0, sizeof(ip));
+    ip.f = f;
+    ip.mask = mask;
+    ip.W = h->p.W;
+    ip.H = h->p.H;
+    ip.bc_left = h->p.bc_left;
+    ip.bc_right = h->p.bc_right;
+    ip.bc_y = h->p.bc_y;
+    ip.k = h->k;
+    for (int done = 0; done < n_steps; done += 2) {
+        ip.ux = ip.uy = ip.rho = nullptr;
+        int rc = inplace_step(h->variant, h->p.storage, ip, false, s);
+        if (rc)
+            return rc;
+        if (done + 2 == n_steps) {
+            ip.ux = ux;
+            ip.uy = uy;
+            ip.rho = rho;
+        }
+        rc = inplace_step(h->variant, h->p.storage, ip, true, s);
+        if (rc)
+            return rc;
+    }
     return LBM_OK;
 }
 

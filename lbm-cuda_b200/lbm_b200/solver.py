@@ -90,6 +90,13 @@ class Solver:
              _ptr(rho), _stream(stream), C.byref(out))
         return out.value
 
+    def run_inplace(self, f, mask, n_steps: int, ux=None, uy=None, rho=None, stream=None) -> None:
+        """lbm_run_inplace: n_steps (even) steps in the single state buffer f."""
+        from . import _ptr, _stream
+
+        call("lbm_run_inplace", self.handle, _ptr(f), _ptr(mask), int(n_steps), _ptr(ux), _ptr(uy), _ptr(rho),
+             _stream(stream))
+
     def diag(self, f, mask, out=None, stream=None):
         """Device tensor [mass, momentum_x, momentum_y] (float64), fixed-order reduction."""
         import torch
