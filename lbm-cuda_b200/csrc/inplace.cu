@@ -176,6 +176,10 @@ __global__ void __launch_bounds__(256) inplace_kernel(const __grid_constant__ In
         inplace_cell<Ph, St, LID, LOCAL>(p, x, y);
 }
 
+#ifndef LBM_INPLACE_MINB
+#define LBM_INPLACE_MINB 3 // CTAs of 256 threads per SM the vector kernel's registers are sized for
+#endif
+
 // Vector kernel (W % 4 == 0, 16-byte aligned planes, mask and macro arrays):
 // four consecutive cells per thread, a warp covers 128 columns of one row, 256
 // columns x 4 rows per CTA.  A warp whose 128 cells are all interior fluid (no
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(256) inplace_kernel(const __grid_constant__ In
 // same thread (the pull of plane k from row r and the push into plane k of row
 // r belong to the cells of row r + c_y(k)).  Other warps run the per-cell code.
 template <class Ph, class St, bool LID, bool LOCAL>
-__global__ void __launch_bounds__(256) inplace_vec_kernel(const __grid_constant__ InplaceParams p)
+__global__ void __launch_bounds__(256, LBM_INPLACE_MINB) inplace_vec_kernel(const __grid_constant__ InplaceParams p)
 {
     using E = typename St::T;
     using V = typename Raw4<E>::type;
