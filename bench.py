@@ -20,8 +20,11 @@ Metric: MLUPS = W*H*physical steps / time, counting every cell as the
 reference does (lbm_mine2.py:106).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--T 1..8] [--storage f32|f16|bf16] [--workload cylinder|batch]
+                    [--T 1..8] [--storage f32|f16|bf16] [--inplace] [--closure smag|mlp]
+                    [--workload cylinder|batch|dropins|c2|c3|c4]
 
+--inplace runs the workload in one state buffer (lbm_run_inplace: the AA
+pattern, one pull-push and one local kernel per pair of steps; T = 1 per kernel).
 --workload batch times 256 independent channel domains of uneven size in one
 persistent launch per T steps (FP16 storage) against one launch per domain.
 --workload c2 runs the cylinder workload for 50 000 steps with drag and lift
