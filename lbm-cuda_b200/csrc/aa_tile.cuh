@@ -13,9 +13,10 @@
 // solid; out-of-domain cells are solid with zero populations, column W-1 is
 // fluid (open outlet ghost).
 //
-// B200 design: one CTA of 512 threads owns a 64 x 32 tile (core (64-2T) x
-// (32-2T) plus a T-cell halo), fetched by a single TMA box [68 x 32 x 9] (plus
-// one for the mask) when the layout allows it.  Threads have a fixed 2-D map
+// B200 design: one CTA of 512 threads owns a 64 x 40 tile (core (64-2T) x
+// (40-2T) plus a T-cell halo; 64 x 32 in the edge band of a split launch),
+// fetched by a single TMA box [68 x SY x 9] (plus one for the mask) when the
+// layout allows it.  Threads have a fixed 2-D map
 // (two warps per tile row, eight rows apart), so phases need no integer
 // division.  After the load the solid test runs once per tile cell and per cell
 // of a one-cell apron (a byte array), and each cell's neighbour code is read

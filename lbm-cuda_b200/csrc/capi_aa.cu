@@ -68,15 +68,22 @@ template <class C> int launch_aa_grid(AaParams p, int nblocks, cudaStream_t s)
 
 template <class Cfg, int MODE> static int aa_split(AaParams p, int T, cudaStream_t s, bool &done);
 
-// Tile shapes: (SX, SY, threads, cells per batch, CTAs per SM).  Shape 2, the
-// default, is a 64 x 32 tile with 512 threads and two CTAs per SM (measured
-// against 32 x 32 / 256 threads / four CTAs, 64 x 32 / 256 threads, 32 x 64 and
-// 64 x 32 / 512 threads with 4-cell batches: fastest at T = 4 and T = 6 on
-// 2048 x 512 and 4096 x 1024); shape 1 is the 32 x 32 tile with four CTAs per SM.
+// Tile shapes: (SX, SY, threads, cells per batch, CTAs per SM).  Measured on the
+// drivers' 2048 x 512 and on 4096 x 1024 (GLUPS, lbm_smemaa_step T = 4 /
+// lbm_blocked_step T = 6): 64 x 40 tiles, 512 threads, one cell per batch, two
+// CTAs per SM (shape 5) are fastest where the tile kernel runs alone (85.2 /
+// 72.3 at 2048 x 512, against 74.9 / 62.4 for 64 x 32 tiles with two-cell
+// batches); on domains of at least 4 M cells, where the tiles only cover the
+// edge band of the split launch, the thinner 64 x 32 tiles with one-cell
+// batches (shape 6) are (86.9 / 71.1 at 4096 x 1024).  Batches of one cell
+// beat two in both (fewer registers per thread under the 64-register cap of
+// two 512-thread CTAs).  Shape 1 (32 x 32, 256 threads, four CTAs per SM) and
+// shape 2 (64 x 32, two-cell batches) stay selectable for experiments.
 template <int VAR, int SHAPE> static int aa_dispatch_shape(const AaParams &p, int T, cudaStream_t s)
 {
-    constexpr int SX = SHAPE == 2 ? 64 : 32, SY = 32, NT = SHAPE == 2 ? 512 : 256, NB = 2;
-    constexpr int MB = SHAPE == 2 ? 2 : 4;
+    constexpr int SX = SHAPE == 1 ? 32 : 64, SY = SHAPE == 5 ? 40 : 32;
+    constexpr int NT = SHAPE == 1 ? 256 : 512, NB = (SHAPE >= 5) ? 1 : 2;
+    constexpr int MB = SHAPE == 1 ? 4 : 2;
     constexpr int MODE = VAR == VARIANT_SMEMAA ? MODE_PRE_SMEMAA : MODE_PRE_POLICY;
     bool done = false;
     int rc = LBM_OK;
@@ -104,12 +111,22 @@ template <int VAR, int SHAPE> static int aa_dispatch_shape(const AaParams &p, in
 
 template <int VAR> static int aa_dispatch(const AaParams &p, int T, cudaStream_t s)
 {
-    static int shape = -1;
-    if (shape < 0) {
-        const char *e = getenv("LBM_AA_SHAPE"); // tuning override for experiments: 1 = 32 x 32 tiles
-        shape = (e && atoi(e) == 1) ? 1 : 2;
+    static int forced = -2;
+    if (forced == -2) {
+        const char *e = getenv("LBM_AA_SHAPE"); // tuning override for experiments
+        forced = e ? atoi(e) : -1;
     }
-    return shape == 1 ? aa_dispatch_shape<VAR, 1>(p, T, s) : aa_dispatch_shape<VAR, 2>(p, T, s);
+    const int shape = forced >= 0 ? forced : ((long long)p.W * p.H >= (4ll << 20) ? 6 : 5);
+    switch (shape) {
+    case 1:
+        return aa_dispatch_shape<VAR, 1>(p, T, s);
+    case 2:
+        return aa_dispatch_shape<VAR, 2>(p, T, s);
+    case 6:
+        return aa_dispatch_shape<VAR, 6>(p, T, s);
+    default:
+        return aa_dispatch_shape<VAR, 5>(p, T, s);
+    }
 }
 
 // Split launch for T = 2, 4, 6 on TMA-aligned buffers: the reference's AA slot
