@@ -75,7 +75,7 @@ struct StoreBF16Dev {
 };
 
 // ---------------------------------------------------------------------------
-// mbarrier and TMA (cp.async.bulk.tensor) wrappers.  No multicast anywhere.
+// mbarrier and TMA (cp.async.bulk.tensor) wrappers.  Every load lands in the issuing CTA's own shared memory.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void *p)
 {
