@@ -112,3 +112,27 @@ def test_general_reduces_to_core4():
     np.testing.assert_allclose(fg, fc, atol=1e-12)
     for a, b in zip(mg, mc):
         np.testing.assert_allclose(a, b, atol=1e-12)
+
+
+def test_poiseuille_profile_is_the_parabola():
+    """Channel with a flat Zou-He inlet, an outflow and half-way bounce-back walls
+    (fluid rows 1 .. H-2, walls at y = 1/2 and y = H - 3/2): downstream of the
+    inlet the velocity profile has the shape of the parabola (y - 1/2)(H - 3/2 - y)
+    of width L = H - 2 (max / mean = 3/2).  The shape, not the level: with a
+    velocity inlet and a zero-gradient outlet (the reference's boundary pair) the
+    channel has no pressure reference, so the density, and with it the mean speed
+    at a given x, drifts."""
+    W, H, u0, nu = 96, 18, 0.04, 0.1
+    g = O.General(W, H, collision="mrt", closure="none", s_nu=1.0 / (3 * nu + 0.5), s_e=1.1, s_eps=1.1, s_q=1.1,
+                  bc_left="zouhe", bc_right="outflow", bc_y="wall", u_in=u0, ref_clamps=False)
+    m = I.channel_mask(W, H)
+    f0 = I.channel_state(W, H, u0=u0, dtype=np.float64)
+    _, mac = g.run(m, f0, 3000)
+    y = np.arange(1, H - 1, dtype=np.float64)
+    shape = (y - 0.5) * (H - 1.5 - y)
+    for x in (40, 70):
+        u = np.asarray(mac[0])[1:H - 1, x]
+        a = u / u.mean()
+        b = shape / shape.mean()
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 0.01, x
+        assert abs(u.max() / u.mean() - 1.5) < 0.01
