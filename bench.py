@@ -304,11 +304,13 @@ def main():
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("bench timed region")
         e0.record(stream)
         for _ in range(args.steps):
             frame()
         e1.record(stream)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
     barrier()
     torch.cuda.synchronize()
     ms = max_over_ranks(e0.elapsed_time(e1))
@@ -368,6 +370,7 @@ def main():
     barrier()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("bench e2e region")
     e2.record(stream)
     for i in range(e2e_steps):
         e2e_step(i)
@@ -375,6 +378,7 @@ def main():
         stream.wait_event(ev_down[j])
     e3.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     e2e_ms = max_over_ranks(e2.elapsed_time(e3))
     e2e_mlups = W * H * e2e_steps * n_launch * T * world / (e2e_ms * 1e3)
     h2d = host_m[0].numel() * host_m[0].element_size()

@@ -278,6 +278,7 @@ extern "C" {
 int lbm_smemaa_step(const uint8_t *mask, const float *f_now, float *f_out, float *ux, float *uy, float *rho, int W,
                     int H, float tau_inv, float u_in, int T, void *stream)
 {
+    NvtxRange nvtx_range("lbm_smemaa_step");
     if (!mask || !f_now || !f_out || !ux || !uy || !rho || f_now == f_out || W < 3 || H < 3)
         return LBM_ERR_ARG;
     if (T < 2 || T > 8 || (T & 1))
@@ -289,6 +290,7 @@ int lbm_smemaa_step(const uint8_t *mask, const float *f_now, float *f_out, float
 int lbm_blocked_step(const uint8_t *mask, const float *f_now, float *f_out, int W, int H, float tau_inv, float u_in,
                      int T, void *stream)
 {
+    NvtxRange nvtx_range("lbm_blocked_step");
     if (!mask || !f_now || !f_out || f_now == f_out || W < 3 || H < 3)
         return LBM_ERR_ARG;
     if (T < 2 || T > 8 || (T & 1))

@@ -460,6 +460,7 @@ int lbm_batch_destroy(lbm_batch *b)
 
 int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in_b)
 {
+    NvtxRange nvtx_range("lbm_batch_run");
     if (!b || n_steps < 0 || T < 0 || T > 8)
         return LBM_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -537,6 +538,7 @@ int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in
 
 int lbm_batch_run_separate(lbm_batch *b, int n_steps, int T, void *stream, int *result_in_b)
 {
+    NvtxRange nvtx_range("lbm_batch_run_separate");
     if (!b || n_steps < 0 || T < 1 || T > 8)
         return LBM_ERR_ARG;
     if (T != 1 && T != 2 && T != 4 && T != 8)

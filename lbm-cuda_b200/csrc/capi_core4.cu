@@ -126,6 +126,7 @@ extern "C" {
 int lbm_core4_step(const uint8_t *mask, const float *f_now, float *f_out, float *ux, float *uy, float *rho, int W,
                    int H, float tau_inv, float u_in, float tau_inv_bnd, void *stream)
 {
+    NvtxRange nvtx_range("lbm_core4_step");
     (void)tau_inv_bnd; // unused by the reference too (lbm_core4.cu:12)
     if (!mask || !f_now || !f_out || !ux || !uy || !rho || f_now == f_out || W < 3 || H < 3 || !(tau_inv > 0.0f))
         return LBM_ERR_ARG;
@@ -136,6 +137,7 @@ int lbm_core4_step(const uint8_t *mask, const float *f_now, float *f_out, float 
 int lbm_core4_run(const uint8_t *mask, float *f_a, float *f_b, float *ux, float *uy, float *rho, int W, int H,
                   float tau_inv, float u_in, int n_steps, int T, void *stream, int *result_in_b)
 {
+    NvtxRange nvtx_range("lbm_core4_run");
     if (!mask || !f_a || !f_b || !ux || !uy || !rho || f_a == f_b || W < 3 || H < 3 || !(tau_inv > 0.0f) ||
         n_steps < 0 || T < 1 || T > 8)
         return LBM_ERR_ARG;

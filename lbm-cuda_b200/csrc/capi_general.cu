@@ -322,6 +322,7 @@ int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *
 int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_steps, int T, float *ux, float *uy,
             float *rho, void *stream, int *result_in_b)
 {
+    NvtxRange nvtx_range("lbm_run");
     if (!h || !f_a || !f_b || !mask || f_a == f_b || n_steps < 0 || T < 1 || T > 8)
         return LBM_ERR_ARG;
     if ((ux || uy || rho) && !(ux && uy && rho))
@@ -378,6 +379,7 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
 int lbm_run_inplace(lbm_handle *h, void *f, const uint8_t *mask, int n_steps, float *ux, float *uy, float *rho,
                     void *stream)
 {
+    NvtxRange nvtx_range("lbm_run_inplace");
     if (!h || !f || !mask || n_steps < 0 || (n_steps & 1))
         return LBM_ERR_ARG;
     if ((ux || uy || rho) && !(ux && uy && rho))

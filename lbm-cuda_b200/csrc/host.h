@@ -4,11 +4,28 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cudaTypedefs.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 #include "lbm_b200.h"
 
 namespace lbm {
+
+// NVTX range around an entry point (header-only NVTX 3: a no-op unless a
+// profiler is attached), so that a capture can be restricted to one call
+// (ncu --nvtx --nvtx-include "lbm_run/").
+struct NvtxRange {
+    explicit NvtxRange(const char *name)
+    {
+        nvtxRangePushA(name);
+    }
+    ~NvtxRange()
+    {
+        nvtxRangePop();
+    }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point, so that the
 // library itself does not link libcuda (it loads on machines without a GPU).

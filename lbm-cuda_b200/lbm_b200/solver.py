@@ -90,6 +90,30 @@ class Solver:
              _ptr(rho), _stream(stream), C.byref(out))
         return out.value
 
+    def run_checked(self, f_a, f_b, mask, n_steps: int, T: int = 4, check_every: int = 1000, ux=None, uy=None,
+                    rho=None, stream=None) -> int:
+        """lbm_run in chunks of check_every steps; after each chunk the FP64 mass
+        and momentum (lbm_diag_fp64) of the state must be finite, else
+        FloatingPointError names the steps in which it stopped being finite (the
+        device-side failure detection: one small reduction and one host read per
+        chunk).  Returns 1 when the final state is in f_b, like run."""
+        import math
+
+        cur, oth = f_a, f_b
+        done = 0
+        while done < n_steps:
+            k = min(int(check_every), n_steps - done)
+            last = done + k == n_steps
+            which = self.run(cur, oth, mask, k, T, *((ux, uy, rho) if last else (None, None, None)), stream=stream)
+            if which:
+                cur, oth = oth, cur
+            d = self.diag(cur, mask, stream=stream).cpu().tolist()
+            if not all(math.isfinite(x) for x in d):
+                raise FloatingPointError(f"the state is not finite after steps {done + 1}..{done + k} "
+                                         f"(mass, momentum = {d})")
+            done += k
+        return 1 if cur is f_b else 0
+
     def run_inplace(self, f, mask, n_steps: int, ux=None, uy=None, rho=None, stream=None) -> None:
         """lbm_run_inplace: n_steps (even) steps in the single state buffer f."""
         from . import _ptr, _stream

@@ -233,3 +233,24 @@ def test_register_wavefront_matches_smem_wavefront(name, T, storage):
         assert rel_l2(fr, ref) < REL_TOL
         for g_, r_ in zip(mr, rmac):
             assert rel_l2(g_[upd], r_[upd]) < REL_TOL
+
+
+def test_checked_run_reports_a_non_finite_state():
+    """Failure detection by fault injection on the host: a NaN written into one
+    fluid cell's populations is reported by the first check after it (an
+    FP64 reduction of mass and momentum), and a clean run passes every check.
+    (Without the reference clamps: fminf / fmaxf return the non-NaN operand, so
+    the clamps replace a NaN population by a bound.)"""
+    W, H = 256, 96
+    kw, kind = CASES["mrt_smag_flat_inlet"]
+    S, _ = make(W, H, **kw)
+    m, f0 = case_inputs(kind, W, H)
+    a, b = dev(f0), dev(f0)
+    md = dev(m)
+    which = S.run_checked(a, b, md, 40, T=2, check_every=10)
+    assert torch.isfinite(b if which else a).all()
+    a, b = dev(f0), dev(f0)
+    ys, xs = np.nonzero(m == 0)
+    a[3, ys[len(ys) // 2], xs[len(xs) // 2]] = float("nan")
+    with pytest.raises(FloatingPointError, match="steps 1..10"):
+        S.run_checked(a, b, md, 40, T=2, check_every=10)
