@@ -100,19 +100,15 @@ __device__ __forceinline__ float2 ld2(const float *p, int)
 {
     return *reinterpret_cast<const float2 *>(p);
 }
+// 16-bit deviations: the weight is added (subtracted on store) on the packed
+// FP32x2 pipe, one instruction for both cells.
 __device__ __forceinline__ float2 ld2(const __half *p, int q)
 {
-    float2 v = __half22float2(*reinterpret_cast<const __half2 *>(p));
-    v.x += wgt(q);
-    v.y += wgt(q);
-    return v;
+    return add2(__half22float2(*reinterpret_cast<const __half2 *>(p)), bc2(wgt(q)));
 }
 __device__ __forceinline__ float2 ld2(const __nv_bfloat16 *p, int q)
 {
-    float2 v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p));
-    v.x += wgt(q);
-    v.y += wgt(q);
-    return v;
+    return add2(__bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(p)), bc2(wgt(q)));
 }
 __device__ __forceinline__ void st2(float *p, float2 v, int)
 {
@@ -120,11 +116,13 @@ __device__ __forceinline__ void st2(float *p, float2 v, int)
 }
 __device__ __forceinline__ void st2(__half *p, float2 v, int q)
 {
-    *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(v.x - wgt(q), v.y - wgt(q));
+    const float2 d = sub2(v, bc2(wgt(q)));
+    *reinterpret_cast<__half2 *>(p) = __floats2half2_rn(d.x, d.y);
 }
 __device__ __forceinline__ void st2(__nv_bfloat16 *p, float2 v, int q)
 {
-    *reinterpret_cast<__nv_bfloat162 *>(p) = __floats2bfloat162_rn(v.x - wgt(q), v.y - wgt(q));
+    const float2 d = sub2(v, bc2(wgt(q)));
+    *reinterpret_cast<__nv_bfloat162 *>(p) = __floats2bfloat162_rn(d.x, d.y);
 }
 
 // Pull of both cells of a lane from the three source rows of the previous
