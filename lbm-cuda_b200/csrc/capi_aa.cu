@@ -16,7 +16,7 @@ int *device_error_word();
 
 template <class C> int launch_aa(AaParams p, cudaStream_t s)
 {
-    static int attr_done[64] = {0};
+    static std::atomic<int> attr_done[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_done[dev]) {
@@ -43,7 +43,7 @@ template <class C> int launch_aa(AaParams p, cudaStream_t s)
 // The tile kernel on an explicit 1-D grid (edge-only launches).
 template <class C> int launch_aa_grid(AaParams p, int nblocks, cudaStream_t s)
 {
-    static int attr_done[64] = {0};
+    static std::atomic<int> attr_done[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr_done[dev]) {
@@ -111,11 +111,10 @@ template <int VAR, int SHAPE> static int aa_dispatch_shape(const AaParams &p, in
 
 template <int VAR> static int aa_dispatch(const AaParams &p, int T, cudaStream_t s)
 {
-    static int forced = -2;
-    if (forced == -2) {
-        const char *e = getenv("LBM_AA_SHAPE"); // tuning override for experiments
-        forced = e ? atoi(e) : -1;
-    }
+    static const int forced = []() { // tuning override for experiments
+        const char *e = getenv("LBM_AA_SHAPE");
+        return e ? atoi(e) : -1;
+    }();
     const int shape = forced >= 0 ? forced : ((long long)p.W * p.H >= (4ll << 20) ? 6 : 5);
     switch (shape) {
     case 1:

@@ -47,7 +47,7 @@ template <class Ph, class St, int T> using RBCfg = RwCfg<T, 1, (T <= 2 ? 1 : 2),
 template <class C> static int rbatch_launch(const BatchDomain *d, const int4 *items, int n_items, int parity,
                                             cudaStream_t s)
 {
-    static int attr[64] = {0};
+    static std::atomic<int> attr[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && !attr[dev]) {

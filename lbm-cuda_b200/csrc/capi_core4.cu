@@ -10,7 +10,7 @@ __device__ int g_error_word;
 
 int *device_error_word()
 {
-    static int *ptr[64] = {nullptr};
+    static std::atomic<int *> ptr[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64)

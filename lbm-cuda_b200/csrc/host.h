@@ -7,6 +7,8 @@
 #include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "lbm_b200.h"
 
 namespace lbm {
@@ -29,18 +31,17 @@ struct NvtxRange {
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point, so that the
 // library itself does not link libcuda (it loads on machines without a GPU).
+// (Looked up once; the static's initialisation is thread-safe.)
 inline PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = []() -> PFN_cuTensorMapEncodeTiled_v12000 {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    }
+            return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        return nullptr;
+    }();
     return fn;
 }
 
@@ -87,10 +88,11 @@ inline int status(cudaError_t e)
     return e == cudaSuccess ? LBM_OK : (int)e;
 }
 
-// Number of SMs of the current device (cached per device).
+// Number of SMs of the current device (cached per device; the per-device
+// caches in this library are atomics, as several host threads may call in).
 inline int sm_count()
 {
-    static int cache[64] = {0};
+    static std::atomic<int> cache[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 0 || dev >= 64)

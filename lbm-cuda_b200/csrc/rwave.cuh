@@ -767,7 +767,7 @@ template <class E> inline bool rwave_ok(const WaveParams &p, int T, int mode, bo
 
 template <class C> int rwave_occupancy()
 {
-    static int cache[64] = {0};
+    static std::atomic<int> cache[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && cache[dev])

@@ -14,7 +14,7 @@ int *device_error_word();
 
 template <class C> int wave_occupancy()
 {
-    static int cache[64] = {0};
+    static std::atomic<int> cache[64];
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev >= 0 && dev < 64 && cache[dev])
