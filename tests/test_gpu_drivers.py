@@ -104,3 +104,24 @@ def test_driver_default_size_run_and_png(kind, tmp_path):
     p = tmp_path / "frame.png"
     d.save_png(str(p))
     np.testing.assert_array_equal(D.read_png(str(p)), d.image_host())
+
+
+def test_driver_command_line(tmp_path):
+    """python -m lbm_b200.drivers: prints the drivers' FPS / MLUPS line and a JSON
+    summary, and writes the last frame as a PNG."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, PYTHONPATH=os.path.join(root, "lbm-cuda_b200"))
+    png = tmp_path / "frame.png"
+    out = subprocess.run([sys.executable, "-m", "lbm_b200.drivers", "--kind", "smemaa", "--W", "512", "--H", "128",
+                          "--frames", "12", "--iters-per-frame", "5", "--png", str(png)],
+                         env=env, capture_output=True, text=True, timeout=300, check=True).stdout
+    assert "[LBM Simulation] FPS:" in out and "MLUPS:" in out
+    res = json.loads(out.strip().splitlines()[-1])
+    assert res["frames"] == 12 and res["physical_steps"] == 12 * 5 * 8 and res["mlups"] > 0
+    img = D.read_png(str(png))
+    assert img.shape == (128, 512, 4) and (img[1:-1, 1:-1, 3] == 255).all()
