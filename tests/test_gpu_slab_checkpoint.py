@@ -69,3 +69,26 @@ def test_checkpoint_resume_continues_exactly(tmp_path, storage):
     w3 = S2.run(f, g, mk, 10, 2)
     assert hdr["step"] == 10
     assert torch.equal((g if w3 else f), straight)
+
+
+@pytest.mark.parametrize("params", [PERIODIC, CHANNEL], ids=["periodic", "channel"])
+def test_graph_replayed_slab_run_equals_per_launch_run(params):
+    """A single-rank slab run replays pairs of (launch, halo copy) from CUDA
+    graphs; calls shorter than two launches take the per-launch loop.  Both must
+    give the same state bit for bit."""
+    W, H = 240, 96
+    m = np.zeros((H, W), np.uint8) if params is PERIODIC else I.random_discs_mask(W, H, 3, 3.0, 6.0, 8)
+    f0 = I.perturbed_state(W, H, 9, amp=0.02)
+    A = SlabSolver(W, H, torch.from_numpy(m), T=2, **params)
+    A.set_state(torch.from_numpy(f0))
+    A.run(40)  # graph replays (10 pairs)
+    B = SlabSolver(W, H, torch.from_numpy(m), T=2, **params)
+    B.set_state(torch.from_numpy(f0))
+    for _ in range(20):
+        B.run(2)  # one launch per call: the per-launch path
+    assert A.steps_done == B.steps_done == 40
+    assert torch.equal(A.gather(), B.gather())
+    A.run(7)  # 1 pair by graph + 1 launch of 2 + 1 launch of 1
+    for n in (2, 2, 2, 1):
+        B.run(n)
+    assert torch.equal(A.gather(), B.gather())
