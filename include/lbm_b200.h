@@ -186,6 +186,13 @@ int lbm_diag_fp64_noalloc(int W, int H, int storage, const void *f, const uint8_
  * d_out: 2 doubles (Fx = drag, Fy = lift) of device memory. */
 int lbm_forces_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d_out, void *stream);
 
+/* Periodic halo refresh in x of one state of `width` columns (no counterpart in
+ * the reference, which has no periodic sides): columns [0, halo) take columns
+ * [width - 2 halo, width - halo) and columns [width - halo, width) take
+ * [halo, 2 halo), in all 9 planes and H rows; one launch.  The single-rank
+ * periodic slab uses it between launches. */
+int lbm_periodic_halo_x(void *f, int width, int H, int halo, int storage, void *stream);
+
 /* Convert a state between storage formats (W*H*9 elements each). */
 int lbm_convert_state(int W, int H, const void *src, int src_storage, void *dst, int dst_storage, void *stream);
 

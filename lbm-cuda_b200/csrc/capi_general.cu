@@ -225,6 +225,24 @@ static Phys make_phys(const lbm_params &p)
     return k;
 }
 
+// Periodic halo refresh of a local domain of `width` columns: columns [0, halo)
+// take the owned columns [width - 2 halo, width - halo), columns [width - halo,
+// width) take [halo, 2 halo); every plane, every row.  Element type of 2 or 4 bytes.
+template <class E> __global__ void periodic_halo_kernel(E *f, int width, int H, int halo, long long plane)
+{
+    const long long n = 9ll * H * (2 * halo);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % (2 * halo));
+        const long long r = i / (2 * halo); // plane * H + row
+        const int q = (int)(r / H), y = (int)(r % H);
+        E *row = f + q * plane + (long long)y * width;
+        if (c < halo)
+            row[c] = row[width - 2 * halo + c];
+        else
+            row[width - halo + (c - halo)] = row[halo + (c - halo)];
+    }
+}
+
 static int grid_for(long long n)
 {
     long long g = (n + 255) / 256;
@@ -439,6 +457,22 @@ int lbm_forces_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d
         final_reduce_kernel<2><<<1, kRedThreads, 0, s>>>(h->partials, kRedBlocks, d_out);
         return status(cudaGetLastError());
     });
+}
+
+int lbm_periodic_halo_x(void *f, int width, int H, int halo, int storage, void *stream)
+{
+    if (!f || H < 1 || halo < 1 || width < 3 * halo)
+        return LBM_ERR_ARG;
+    if (storage < LBM_STORE_F32 || storage > LBM_STORE_BF16DEV)
+        return LBM_ERR_ARG;
+    const long long n = 9ll * H * 2 * halo;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const long long plane = (long long)width * H;
+    if (storage == LBM_STORE_F32)
+        periodic_halo_kernel<float><<<grid_for(n), 256, 0, s>>>(static_cast<float *>(f), width, H, halo, plane);
+    else
+        periodic_halo_kernel<uint16_t><<<grid_for(n), 256, 0, s>>>(static_cast<uint16_t *>(f), width, H, halo, plane);
+    return status(cudaGetLastError());
 }
 
 int lbm_convert_state(int W, int H, const void *src, int src_storage, void *dst, int dst_storage, void *stream)

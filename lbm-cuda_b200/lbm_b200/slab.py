@@ -158,6 +158,13 @@ class SlabSolver:
         lay, h = self.lay, self.halo
         n = lay.x1 - lay.x0
         left, right = self._neighbours()
+        if self.world == 1 and left is not None and f.is_cuda and lay.left == lay.right == h:
+            # periodic single rank on the GPU: both halos in one launch
+            from . import _ptr, _stream
+            from ._lib import call
+
+            call("lbm_periodic_halo_x", _ptr(f), int(f.shape[2]), self.H, h, int(self.storage), _stream(None))
+            return
         send_l = f[:, :, lay.left:lay.left + h].contiguous() if left is not None else None
         send_r = f[:, :, lay.left + n - h:lay.left + n].contiguous() if right is not None else None
         recv_l = f.new_empty((9, self.H, h)) if left is not None else None
