@@ -77,6 +77,9 @@ def test_solver_calls_refuse_bad_arguments(lib):
     assert lib.lbm_forces_fp64(nul, P, P, P, None) == ERR_ARG
     assert lib.lbm_destroy(nul) == ERR_ARG
     assert lib.lbm_convert_state(64, 32, P, 9, P2, 0, None) == ERR_ARG
+    assert lib.lbm_periodic_halo_x(P, 64, 32, 0, 0, None) == ERR_ARG  # no halo
+    assert lib.lbm_periodic_halo_x(P, 10, 32, 4, 0, None) == ERR_ARG  # narrower than three halos
+    assert lib.lbm_periodic_halo_x(P, 64, 32, 2, 5, None) == ERR_ARG  # unknown storage
     # the learned-closure training calls
     assert lib.lbm_mlp_forward(nul, P, P, 10, None) == ERR_ARG
     assert lib.lbm_mlp_grad(P, P, P, nul, 0, P, P, P, C.c_size_t(1 << 20), None) == ERR_ARG
