@@ -132,7 +132,8 @@ typedef struct lbm_handle lbm_handle;
 void lbm_params_default(lbm_params *p, int W, int H);
 
 /* Validate the parameters and allocate the handle and its small reduction
- * scratch (the only entry point that allocates); lbm_destroy frees them. */
+ * scratch (the only entry point that allocates device memory); lbm_destroy
+ * frees them and lbm_run's cached graph. */
 int lbm_create(const lbm_params *p, lbm_handle **out);
 int lbm_destroy(lbm_handle *h);
 
@@ -145,7 +146,12 @@ int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *
 /* n_steps pull steps in ping-pong order starting from f_a, fused T per launch
  * (1 <= T <= 8).  The stored state is post-collision populations (the
  * lbm_core4.cu convention).  u, v, rho of the last step are written when the
- * pointers are non-NULL.  *result_in_b = 1 when the final state is in f_b. */
+ * pointers are non-NULL.  *result_in_b = 1 when the final state is in f_b.
+ * When at least three whole pairs of T-step launches precede the last launch,
+ * the handle captures one pair as a CUDA graph (kept for the same f_a, f_b,
+ * mask and T until another key or lbm_destroy) and replays it, so a small
+ * domain pays one graph launch per pair; the results are bit-identical to the
+ * plain launches, which a stream under capture by the caller always gets. */
 int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_steps, int T, float *ux, float *uy,
             float *rho, void *stream, int *result_in_b);
 
