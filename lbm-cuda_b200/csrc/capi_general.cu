@@ -6,18 +6,27 @@
 
 #include "dispatch.cuh"
 
+namespace lbm {
+struct PairGraph {
+    cudaGraphExec_t exec;
+    const void *a, *b, *mask;
+    int T;
+    unsigned long long last_use;
+};
+} // namespace lbm
+
 struct lbm_handle {
     lbm_params p;
     lbm::Phys k;
     int variant;      // VAR_* compile-time physics variant
     double *partials; // reduction scratch: kRedBlocks x 3 doubles
-    // lbm_run's CUDA graph of one ping-pong pair of launches (f_a -> f_b -> f_a),
-    // captured on a private stream for the buffers, mask and depth of `g_key`
+    // lbm_run's CUDA graphs of one ping-pong pair of launches (a -> b -> a), captured
+    // on a private stream; two slots, so that a caller alternating (f_a, f_b) and
+    // (f_b, f_a) keeps both
     cudaStream_t cap;
-    cudaGraphExec_t g_exec;
-    const void *g_a, *g_b, *g_mask;
-    int g_T;
-    std::atomic<int> g_busy; // held by the lbm_run call using the graph (others launch plainly)
+    lbm::PairGraph graphs[2];
+    unsigned long long uses;
+    std::atomic<int> g_busy; // held by the lbm_run call using the graphs (others launch plainly)
 };
 
 namespace lbm {
@@ -321,8 +330,9 @@ int lbm_destroy(lbm_handle *h)
 {
     if (!h)
         return LBM_ERR_ARG;
-    if (h->g_exec)
-        cudaGraphExecDestroy(h->g_exec);
+    for (auto &g : h->graphs)
+        if (g.exec)
+            cudaGraphExecDestroy(g.exec);
     if (h->cap)
         cudaStreamDestroy(h->cap);
     cudaError_t e = cudaFree(h->partials);
@@ -386,41 +396,59 @@ static int run_launch(lbm_handle *h, void *src, void *dst, const uint8_t *mask, 
     return LBM_ERR_ARG;
 }
 
+// The cached graph of the pair a -> b -> a, or null.
+static PairGraph *find_pair(lbm_handle *h, const void *a, const void *b, const void *mask, int T)
+{
+    for (auto &g : h->graphs)
+        if (g.exec && g.a == a && g.b == b && g.mask == mask && g.T == T) {
+            g.last_use = ++h->uses;
+            return &g;
+        }
+    return nullptr;
+}
+
 // Captures the pair a -> b -> a of T-step launches on the handle's private
-// stream and instantiates it (the launches are recorded, not run).
-static int capture_pair(lbm_handle *h, void *a, void *b, const uint8_t *mask, int T)
+// stream into the least recently used slot and instantiates it (the launches
+// are recorded, not run).
+static PairGraph *capture_pair(lbm_handle *h, void *a, void *b, const uint8_t *mask, int T)
 {
     cudaError_t e;
-    if (!h->cap && (e = cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking)) != cudaSuccess)
-        return status(e);
-    if (h->g_exec) {
-        cudaGraphExecDestroy(h->g_exec);
-        h->g_exec = nullptr;
+    if (!h->cap && cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
     }
-    if ((e = cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
-        return status(e);
+    PairGraph *slot = &h->graphs[0];
+    for (auto &g : h->graphs)
+        if (!g.exec || g.last_use < slot->last_use)
+            slot = &g;
+    if (slot->exec) {
+        cudaGraphExecDestroy(slot->exec);
+        slot->exec = nullptr;
+    }
+    if (cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
     int rc = run_launch(h, a, b, mask, T, nullptr, nullptr, nullptr, h->cap);
     if (!rc)
         rc = run_launch(h, b, a, mask, T, nullptr, nullptr, nullptr, h->cap);
     cudaGraph_t g = nullptr;
     e = cudaStreamEndCapture(h->cap, &g);
-    if (rc || e != cudaSuccess || !g) {
-        if (g)
-            cudaGraphDestroy(g);
+    if (!rc && e == cudaSuccess && g)
+        e = cudaGraphInstantiate(&slot->exec, g, 0);
+    if (g)
+        cudaGraphDestroy(g);
+    if (rc || e != cudaSuccess || !slot->exec) {
+        slot->exec = nullptr;
         cudaGetLastError();
-        return rc ? rc : status(e == cudaSuccess ? cudaErrorUnknown : e);
+        return nullptr;
     }
-    e = cudaGraphInstantiate(&h->g_exec, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) {
-        h->g_exec = nullptr;
-        return status(e);
-    }
-    h->g_a = a;
-    h->g_b = b;
-    h->g_mask = mask;
-    h->g_T = T;
-    return LBM_OK;
+    slot->a = a;
+    slot->b = b;
+    slot->mask = mask;
+    slot->T = T;
+    slot->last_use = ++h->uses;
+    return slot;
 }
 
 } // namespace lbm
@@ -453,9 +481,8 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
     int idle = 0;
     if (graphs && pairs >= 1 && cudaStreamIsCapturing(s, &cs) == cudaSuccess && cs == cudaStreamCaptureStatusNone &&
         h->g_busy.compare_exchange_strong(idle, 1)) {
-        const bool have = h->g_exec && h->g_a == f_a && h->g_b == f_b && h->g_mask == mask && h->g_T == T;
-        bool ok = have;
-        if (!have && pairs >= 3) {
+        PairGraph *pg = find_pair(h, f_a, f_b, mask, T);
+        if (!pg && pairs >= 3) {
             if ((rc = run_launch(h, f_a, f_b, mask, T, nullptr, nullptr, nullptr, s)) ||
                 (rc = run_launch(h, f_b, f_a, mask, T, nullptr, nullptr, nullptr, s))) {
                 h->g_busy = 0;
@@ -464,11 +491,11 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
             done += 2 * T;
             launches += 2;
             --pairs;
-            ok = capture_pair(h, f_a, f_b, mask, T) == LBM_OK; // on failure: plain launches below
+            pg = capture_pair(h, f_a, f_b, mask, T); // on failure: plain launches below
         }
-        if (ok) {
+        if (pg) {
             for (int i = 0; i < pairs; ++i) {
-                cudaError_t e = cudaGraphLaunch(h->g_exec, s);
+                cudaError_t e = cudaGraphLaunch(pg->exec, s);
                 if (e != cudaSuccess) {
                     h->g_busy = 0;
                     return status(e);

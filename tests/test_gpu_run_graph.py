@@ -100,3 +100,25 @@ def test_graph_is_skipped_inside_a_caller_capture():
     del graph
     G.close()
     S.close()
+
+
+def test_alternating_buffer_order_keeps_both_graphs():
+    """A caller that swaps (f_a, f_b) after each call of an odd launch count
+    alternates between two cached graphs; the state matches plain launches."""
+    c = CASES["channel_discs"]
+    W, H = c["W"], c["H"]
+    m = dev(_mask("channel_discs", W, H))
+    f0 = I.perturbed_state(W, H, 6, amp=0.02)
+    S = SV.Solver(W, H, **c["kw"])
+    G = SV.Solver(W, H, **c["kw"])
+    x, y = dev(f0), dev(f0)
+    p, q = dev(f0), dev(f0)
+    for _ in range(5):
+        w = G.run(x, y, m, 42, 2)  # 21 launches: the result is in the second buffer
+        assert w == 1
+        x, y = y, x
+        r = _plain(S, p, q, m, 42, 2, (None, None, None))
+        p, q = (r, p) if r is q else (r, q)
+        assert np.array_equal(host(x), host(p))
+    G.close()
+    S.close()
