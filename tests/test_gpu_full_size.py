@@ -14,7 +14,9 @@
   rounding); a flat-inlet channel with a cylinder centred between the walls
   stays mirror-symmetric; a periodic 1024^2 box of decaying turbulence keeps its
   mass and momentum; a periodic box shifted by whole columns and rows gives the
-  shifted result bit for bit."""
+  shifted result bit for bit.
+* The 256-domain batch (sizes U[64, 1024]^2): every domain against the oracle
+  (FP32), and the benchmark's FP16 batch against one launch per domain."""
 import numpy as np
 import pytest
 import torch
@@ -174,3 +176,65 @@ def test_periodic_box_is_translation_equivariant():
     err = rel_l2(r1, np.roll(r0, (dy, dx), axis=(1, 2)))
     assert err == 0.0, err
     S.close()
+
+
+def _batch_256(storage, tdt, perturbed):
+    """The 256-domain batch configuration: Nx, Ny ~ U[64, 1024], 1-4 discs of
+    radius 4-32, inlet u ~ U[0.02, 0.08] (seeded as the benchmark builds it)."""
+    rng = np.random.default_rng(1234)
+    doms, hosts = [], []
+    for i in range(256):
+        w, h = int(rng.integers(64, 1025)), int(rng.integers(64, 1025))
+        m = I.random_discs_mask(w, h, int(rng.integers(1, 5)), 4.0, min(32.0, h / 4), 5000 + i)
+        u_in = float(rng.uniform(0.02, 0.08))
+        pitch = (w + 15) // 16 * 16
+        mk = torch.zeros((h, pitch), dtype=torch.uint8, device="cuda")
+        mk[:, :w] = dev(m)
+        f0 = I.perturbed_state(w, h, 7000 + i, amp=0.02) if perturbed else None
+        fa = torch.zeros((9, h, pitch), dtype=tdt, device="cuda")
+        if perturbed:
+            fa[:, :, :w] = dev(f0)
+        doms.append(dict(W=w, H=h, pitch=pitch, mask_pitch=pitch, f_a=fa, f_b=fa.clone(), mask=mk, u_in=u_in))
+        hosts.append((m, f0, u_in))
+    return doms, hosts
+
+
+def test_batch_of_256_domains_vs_oracle():
+    """Every domain of the full 256-domain batch (FP32 storage here, from
+    perturbed states) against the oracle run of that domain alone."""
+    from lbm_b200.batch import Batch
+
+    doms, hosts = _batch_256(SV.STORE_F32, torch.float32, True)
+    B = Batch(doms, storage=SV.STORE_F32, cs_smag=0.1, s_nu=1.0 / TAU)
+    n = 9
+    which = B.run(n, 4)
+    worst = 0.0
+    for d, (m, f0, u_in) in zip(doms, hosts):
+        W = d["W"]
+        out = host((d["f_b"] if which else d["f_a"])[:, :, :W].contiguous())
+        G = O.General(W, d["H"], cs=0.1, s_nu=1.0 / TAU, u_in=u_in)
+        ref, _ = G.run(m, f0, n)
+        worst = max(worst, rel_l2(out, ref))
+    assert worst < REL_TOL, worst
+
+
+def test_batch_of_256_domains_fp16_equals_separate_launches():
+    """The benchmark's batch exactly (FP16 deviations, fluid at rest): one
+    launch per T steps for all domains equals one launch per domain."""
+    from lbm_b200.batch import Batch
+
+    doms1, _ = _batch_256(SV.STORE_F16DEV, torch.float16, False)
+    doms2, _ = _batch_256(SV.STORE_F16DEV, torch.float16, False)
+    B1 = Batch(doms1, storage=SV.STORE_F16DEV, cs_smag=0.1, s_nu=1.0 / TAU)
+    B2 = Batch(doms2, storage=SV.STORE_F16DEV, cs_smag=0.1, s_nu=1.0 / TAU)
+    w1 = B1.run(40, 4)
+    w2 = B2.run_separate(40, 4)
+    assert w1 == w2
+    wts = I.WEIGHTS[:, None, None].astype(np.float32)
+    worst = 0.0
+    for d1, d2 in zip(doms1, doms2):
+        W = d1["W"]
+        a = host((d1["f_b"] if w1 else d1["f_a"])[:, :, :W].float()) + wts
+        b = host((d2["f_b"] if w2 else d2["f_a"])[:, :, :W].float()) + wts
+        worst = max(worst, rel_l2(a, b))
+    assert worst < REL_TOL, worst
