@@ -74,11 +74,13 @@ def _driver_case(W=2048, H=512):
     return mask, f0
 
 
-def test_core4_vs_reference_kernel_driver_size():
+@pytest.mark.parametrize("W,H", [(2048, 512), (4096, 1024)])
+def test_core4_vs_reference_kernel_driver_size(W, H):
+    """The drivers' 2048 x 512 case, and the same set-up at 4096 x 1024 (a
+    D = 128 disc at (1024, 512): the cylinder channel's geometry)."""
     lib = ref_lib("libref_core4.so")
     if lib is None:
         pytest.skip("oracle/_ref not built")
-    W, H = 2048, 512
     mask, f0 = _driver_case(W, H)
     m = dev(mask)
     a, b = dev(f0), dev(f0)
@@ -152,13 +154,15 @@ def test_blocked_vs_oracle(W, H, T):
         assert rel_l2(host(g), r) < REL_TOL
 
 
+@pytest.mark.parametrize("W,H", [(2048, 512), (4096, 1024)])
 @pytest.mark.parametrize("libname,kind", [("libref_smemaa.so", "smemaa"), ("libref_policy.so", "policy"),
                                           ("libref_endfused.so", "endfused")])
-def test_blocked_vs_reference_kernel_driver_size(libname, kind):
+def test_blocked_vs_reference_kernel_driver_size(libname, kind, W, H):
+    """At 4096 x 1024 (4.2 M cells) the drop-ins take the split launch (edge
+    tiles beside the interior register wavefront)."""
     lib = ref_lib(libname)
     if lib is None:
         pytest.skip("oracle/_ref not built")
-    W, H = 2048, 512
     mask, f0 = _driver_case(W, H)
     T = lib.ref_T()
     n = 8
