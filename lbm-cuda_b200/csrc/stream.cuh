@@ -234,11 +234,14 @@ template <class C> __global__ void __launch_bounds__(128, 4) stream_kernel(const
         mrx[d] = redge ? mr[d] : right;
     }
 
-    // Interior cells: rows 1..H-2 (walls and periodic rows take the generic
-    // path), columns 1..W-3 (no inlet, outlet source or ghost), no solid cell
-    // in the 3x3 neighbourhood of any of the four cells.
+    // Interior cells: rows 1..H-2 (every row when y is periodic: the row loads
+    // above already wrapped, so the first and last rows pull like any other and
+    // the arithmetic does not depend on the row), columns 1..W-3 (no inlet,
+    // outlet source or ghost), no solid cell in the 3x3 neighbourhood of any of
+    // the four cells.
     const uint32_t any_solid = mw[0] | mw[1] | mw[2] | mlx[0] | mlx[1] | mlx[2] | mrx[0] | mrx[1] | mrx[2];
-    const bool interior = xok && y >= 1 && y <= H - 2 && x4 >= 1 && x4 + 3 <= W - 3 && any_solid == 0;
+    const bool yin = pyper ? (y >= 0 && y < H) : (y >= 1 && y <= H - 2);
+    const bool interior = xok && yin && x4 >= 1 && x4 + 3 <= W - 3 && any_solid == 0;
     const bool fast = __all_sync(0xffffffffu, interior);
 
     float out[9][4], ro[4], uo[4], vo[4];

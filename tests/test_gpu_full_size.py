@@ -16,7 +16,8 @@
   mass and momentum; a periodic box shifted by whole columns and rows gives the
   shifted result bit for bit.
 * The 256-domain batch (sizes U[64, 1024]^2): every domain against the oracle
-  (FP32), and the benchmark's FP16 batch against one launch per domain."""
+  (FP32), and the benchmark's FP16 batch against one launch per domain.
+* The largest domain: 268 M cells, where plane offsets pass 2^31 elements."""
 import numpy as np
 import pytest
 import torch
@@ -238,3 +239,35 @@ def test_batch_of_256_domains_fp16_equals_separate_launches():
         b = host((d2["f_b"] if w2 else d2["f_a"])[:, :, :W].float()) + wts
         worst = max(worst, rel_l2(a, b))
     assert worst < REL_TOL, worst
+
+
+@pytest.mark.parametrize("storage,T", [(SV.STORE_F32, 1), (SV.STORE_F32, 2), (SV.STORE_F32, 4),
+                                       (SV.STORE_F16DEV, 2), (SV.STORE_F32, "inplace")])
+def test_largest_domain_repeats_the_small_result(storage, T):
+    """A 4096 x 65536 channel (268 M cells: plane offsets pass 2^31 elements),
+    periodic in y, built as 64 copies of a 4096 x 1024 channel stacked in y.
+    Every copy sees the neighbourhood of the small periodic domain, so after 8
+    steps each copy equals the small domain's result bit for bit."""
+    W, h, reps, n = 4096, 1024, 64, 8
+    m = I.random_discs_mask(W, h, 6, 8.0, 40.0, 21)
+    m[0, :] = 0
+    m[h - 1, :] = 0
+    kw = dict(bc_y=SV.BC_PERIODIC, bc_left=SV.BC_ZOUHE, ref_clamps=0)  # flat inlet: no y-dependent ramp
+    tdt = torch.float32 if storage == SV.STORE_F32 else torch.float16
+    f0 = torch.empty((9, h, W), dtype=tdt, device="cuda")
+    SV.convert_state(dev(I.perturbed_state(W, h, 23, amp=0.02)), SV.STORE_F32, f0, storage)
+
+    def run(S, mask, a):
+        if T == "inplace":
+            S.run_inplace(a, mask, n)
+            return a
+        b = a.clone()
+        which = S.run(a, b, mask, n, T)
+        return b if which else a
+
+    small = run(_solver(W, h, storage=storage, **kw), dev(m), f0.clone())
+    S = _solver(W, h * reps, storage=storage, **kw)
+    big = run(S, dev(np.tile(m, (reps, 1))), f0.repeat(1, reps, 1))
+    torch.cuda.synchronize()
+    assert torch.equal(big.view(9, reps, h, W), small.unsqueeze(1).expand(9, reps, h, W))
+    S.close()
