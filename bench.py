@@ -29,9 +29,10 @@ pattern, one pull-push and one local kernel per pair of steps; T = 1 per kernel)
 persistent launch per T steps (FP16 storage) against one launch per domain.
 --workload c2 runs the cylinder workload for 50 000 steps with drag and lift
 sampled every 100 steps (mean drag coefficient, RMS lift, Strouhal number).
---workload c3 runs the 8192 x 2048 cylinder (D = 256, Re = 20 000) in FP32, FP16
-and BF16 deviation storage to 1k / 10k / 50k steps and reports the 16-bit runs'
-velocity error against the FP32 run, and each format's MLUPS at that size.
+--workload c3 runs the 8192 x 2048 cylinder (D = 256, Re = 20 000) in FP64 (the
+judge: double storage and arithmetic), FP32, FP16 and BF16 deviation storage to
+1k / 10k / 50k steps and reports each format's velocity error against the FP64
+run, and each format's MLUPS at that size.
 --workload c4 runs decaying periodic turbulence at 1024^2 with no closure,
 Smagorinsky and the learned closure (FP32 and FP16 storage) against a 4096^2
 judge filtered 4x, the network trained on the GPU on another seed's judge, and
@@ -201,6 +202,8 @@ def main():
     ap.add_argument("--workload", choices=["cylinder", "batch", "dropins", "c2", "c3", "c4"], default="cylinder")
     ap.add_argument("--c2-steps", type=int, default=50000, help="c2: physical steps")
     ap.add_argument("--c2-out", default=None, help="c2: CSV file for the drag / lift series")
+    ap.add_argument("--c3-marks", default=None, help="c3: comma-separated checkpoints (default 1000,10000,50000)")
+    ap.add_argument("--c3-out", default=None, help="c3: also write the result line to this JSON file")
     ap.add_argument("--c4-n", type=int, default=1024, help="c4: coarse grid (the judge is 4x finer)")
     ap.add_argument("--c4-steps", type=int, default=20000, help="c4: coarse steps")
     ap.add_argument("--c4-epochs", type=int, default=30, help="c4: training epochs")
@@ -572,21 +575,26 @@ def run_c2(args, torch):
 
 def run_c3(args, torch):
     """8192 x 2048 channel past a D = 256 cylinder at (2048, 1024), Re = 20 000
-    (u = 0.05, nu = 6.4e-4, Cs = 0.1), FP32 / FP16 / BF16 storage, T = 2."""
+    (u = 0.05, nu = 6.4e-4, Cs = 0.1, the reference's clamps), from rest with
+    u_y noise +-1e-4 (seed 0).  FP64 storage and arithmetic (one step per
+    launch) is the judge; FP32, FP16-deviation and BF16-deviation storage run
+    at T = 2.  Reports each format's velocity relative L2 against the FP64 run
+    over the fluid cells at the checkpoints (1k, 10k, 50k steps), and MLUPS."""
     from lbm_b200 import init as I
     from lbm_b200 import solver as SV
 
     Wc, Hc = 8192, 2048
     mask = torch.from_numpy(I.cylinder_mask(Wc, Hc, 2048, 1024, 256, value=I.OBSTACLE)).cuda()
     f0 = torch.from_numpy(I.channel_state(Wc, Hc, u0=0.0, noise=1e-4, seed=0)).cuda()
-    marks = [1000, 10000, 50000] if args.steps >= 3 else [1000]
+    marks = [int(x) for x in args.c3_marks.split(",")] if args.c3_marks else [1000, 10000, 50000]
     T = 2
     vel, mlups = {}, {}
-    for name, st in (("f32", SV.STORE_F32), ("f16", SV.STORE_F16DEV), ("bf16", SV.STORE_BF16DEV)):
+    formats = (("f64", SV.STORE_F64), ("f32", SV.STORE_F32), ("f16", SV.STORE_F16DEV), ("bf16", SV.STORE_BF16DEV))
+    for name, st in formats:
         S = SV.Solver(Wc, Hc, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU, storage=st)
         a = S.new_state()
         SV.convert_state(f0, SV.STORE_F32, a, st)
-        b = torch.empty_like(a)
+        b = a.clone()
         mac = [torch.empty((Hc, Wc), device="cuda") for _ in range(3)]
         done, vel[name] = 0, []
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -603,19 +611,28 @@ def run_c3(args, torch):
             vel[name].append(torch.stack([mac[0], mac[1]]).cpu())
         mlups[name] = round(Wc * Hc * done / (ms * 1e3), 1)
         del S, a, b
+        torch.cuda.empty_cache()
     fl = (mask == 0).cpu()
-    err = {}
-    for name in ("f16", "bf16"):
-        err[name] = []
-        for v, r in zip(vel[name], vel["f32"]):
+
+    def rel(name, judge):
+        out = []
+        for v, r in zip(vel[name], vel[judge]):
             d = (v - r)[:, fl].double()
-            err[name].append(float(d.norm() / r[:, fl].double().norm()))
-    return {"metric": "MLUPS", "value": mlups["f16"], "unit": "MLUPS", "n_gpus": 1, "steps": marks[-1],
-            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f16-deviation storage, f32 math", "data": "synthetic",
+            out.append(float(d.norm() / r[:, fl].double().norm()))
+        return out
+
+    err64 = {name: rel(name, "f64") for name in ("f32", "f16", "bf16")}
+    err32 = {name: rel(name, "f32") for name in ("f16", "bf16")}
+    line = {"metric": "velocity rel. L2 vs FP64", "value": err64["f16"][0], "unit": "relative L2", "n_gpus": 1,
+            "steps": marks[-1], "warmup": 0, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f16-deviation storage, f32 math (value: FP16 at the first checkpoint)", "data": "synthetic",
             "config": {"workload": f"cylinder channel {Wc}x{Hc}, D=256 at (2048,1024), Re=20000, Cs={CS}, "
-                                   f"u={U_IN}, T={T}", "checkpoints": marks},
-            "mlups_by_storage": mlups, "velocity_rel_l2_vs_f32": err}
+                                   f"u={U_IN}, clamps, T={T} (FP64: one step per launch)", "checkpoints": marks},
+            "velocity_rel_l2_vs_f64": err64, "velocity_rel_l2_vs_f32": err32, "mlups_by_storage": mlups}
+    if args.c3_out:
+        with open(args.c3_out, "w") as fh:
+            json.dump(line, fh, indent=1)
+    return line
 
 
 def run_c4(args, torch):

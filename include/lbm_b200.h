@@ -14,7 +14,10 @@
  *     reference drivers do (lbm_mine2.py:75-81);
  *   - the return value is 0 on success, the cudaError_t of a failing CUDA call
  *     (1..999), or one of the LBM_ERR_* validation codes below.  The reference
- *     kernels return nothing; their launch errors surface asynchronously.
+ *     kernels return nothing; their launch errors surface asynchronously;
+ *   - the library keeps a few per-device objects for the life of the process (the
+ *     addresses of its __device__ arrays, TMA entry points, side streams); a
+ *     device reset (cudaDeviceReset) while the library is loaded is not supported.
  */
 #ifndef LBM_B200_H
 #define LBM_B200_H
@@ -37,6 +40,8 @@ extern "C" {
 #define LBM_STORE_F32 0
 #define LBM_STORE_F16DEV 1  /* IEEE half of f_q - w_q, FP32 arithmetic */
 #define LBM_STORE_BF16DEV 2 /* bfloat16 of f_q - w_q, FP32 arithmetic */
+#define LBM_STORE_F64 3     /* IEEE double and FP64 arithmetic, one step per launch: the
+                               high-precision judge of the other formats (general solver only) */
 
 /* Mask byte values of the general solver (the drop-ins treat nonzero as solid). */
 #define LBM_MASK_FLUID 0
@@ -144,16 +149,26 @@ size_t lbm_state_bytes(const lbm_handle *h);
 int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *ux, const float *uy, void *stream);
 
 /* n_steps pull steps in ping-pong order starting from f_a, fused T per launch
- * (1 <= T <= 8).  The stored state is post-collision populations (the
- * lbm_core4.cu convention).  u, v, rho of the last step are written when the
- * pointers are non-NULL.  *result_in_b = 1 when the final state is in f_b.
- * When at least three whole pairs of T-step launches precede the last launch,
- * the handle captures one pair as a CUDA graph (kept for the same f_a, f_b,
- * mask and T until another key or lbm_destroy) and replays it, so a small
- * domain pays one graph launch per pair; the results are bit-identical to the
- * plain launches, which a stream under capture by the caller always gets. */
+ * (1 <= T <= 8; FP64 storage: one step per launch whatever T).  The stored
+ * state is post-collision populations (the lbm_core4.cu convention).  u, v, rho
+ * of the last step are written when the pointers are non-NULL.  *result_in_b =
+ * 1 when the final state is in f_b.
+ * Graph cache: when at least three whole pairs of T-step launches precede the
+ * last launch, the handle captures one pair as a CUDA graph and replays it, so
+ * a small domain pays one graph launch per pair; the results are bit-identical
+ * to the plain launches, which a stream under capture by the caller always
+ * gets.  Up to two graphs are kept, keyed by the ADDRESSES of f_a, f_b and mask
+ * and by T (the handle's W, H and parameters are fixed), until another key
+ * evicts them, lbm_run_graph_reset or lbm_destroy.  A caller that frees its
+ * state buffers and allocates new ones (which may reuse the same addresses)
+ * calls lbm_run_graph_reset first; LBM_RUN_GRAPH=0 in the environment turns
+ * the cache off. */
 int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_steps, int T, float *ux, float *uy,
             float *rho, void *stream, int *result_in_b);
+
+/* Drops lbm_run's cached graphs (no counterpart in the reference).  Returns
+ * LBM_ERR_ARG while an lbm_run on another thread is replaying them. */
+int lbm_run_graph_reset(lbm_handle *h);
 
 /* n_steps steps in ONE state buffer (no counterpart in the reference, whose
  * drivers ping-pong two buffers, lbm_mine2.py:77-80): half the state memory of
@@ -238,8 +253,6 @@ int lbm_batch_run_separate(lbm_batch *b, int n_steps, int T, void *stream, int *
  * (states end in f_a).  Synchronous. */
 int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk);
 
-/* Read (and optionally clear) the device error word of the current device:
- * bit 0 = a bounded device-side wait gave up.  Synchronises the device. */
 /* ------------------------------------------------------------------------
  * Learned closure (no reference counterpart): a 5 -> 32 -> 32 -> 1 MLP (ReLU,
  * ReLU, softplus) maps per-cell features to an eddy viscosity nu_t >= 0; the
@@ -272,7 +285,19 @@ int lbm_mlp_adam(float *params, const float *grad, float *m, float *v, int step,
  * in_scale[5] before the first layer and nu_t = out_scale * softplus(z). */
 int lbm_mlp_pack(const float *params, const float *in_scale, float out_scale, void *packed, void *stream);
 
+/* Read (and optionally clear) the device error word of the current device:
+ * bit 0 = a bounded device-side wait gave up (the kernel then stopped its work
+ * and returned; the launch itself reports success).  Synchronises the device. */
 int lbm_device_error_flags(int *flags, int clear);
+
+/* Self-test of the give-up path of the bounded device-side waits (no reference
+ * counterpart): one CTA initialises an mbarrier and waits on it with a limit of
+ * limit_cycles SM cycles (1 .. 2^31).  With arrive = 0 nothing arrives and no
+ * copy is issued, so the wait runs out, the kernel sets bit 0 of the device
+ * error word and returns; with arrive = 1 the CTA arrives first and the wait
+ * succeeds.  d_cycles (optional, one device int64) receives the cycles the
+ * wait took.  Nothing faults or hangs either way. */
+int lbm_selftest_wait_timeout(long long limit_cycles, int arrive, long long *d_cycles, void *stream);
 
 /* Human-readable text for a status code (static storage). */
 const char *lbm_error_string(int status);

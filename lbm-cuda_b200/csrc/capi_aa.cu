@@ -4,8 +4,6 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include <mutex>
-
 #include "aa_tile.cuh"
 #include "host.h"
 #include "rwave.cuh"
@@ -135,30 +133,54 @@ template <int VAR> static int aa_dispatch(const AaParams &p, int T, cudaStream_t
 // edge band, and the register wavefront kernel in pre-collision mode on the
 // interior rectangle (tile-aligned, at least T + 2 cells from every edge), where
 // both give the same values.  LBM_AA_SPLIT=0 runs the tile kernel everywhere.
-// Side stream and events per device for running the edge-band kernel beside the
-// interior kernel (fork on an event of the caller's stream, join on another);
-// event waits keep the pair capturable into a CUDA graph.
+// Side stream and events for running the edge-band kernel beside the interior
+// kernel (fork on an event of the caller's stream, join on another); event waits
+// keep the pair capturable into a CUDA graph.  They are owned by the calling host
+// thread, one set per device: two threads splitting at the same time never
+// re-record each other's fork event between its record and the side stream's
+// wait, and a thread capturing a graph never pulls another thread's edge-band
+// launch into it (a side stream that joined a capture stays in it until the
+// capture ends).  The set is released when its thread exits.
 struct SplitStreams {
     cudaStream_t side = nullptr;
     cudaEvent_t fork = nullptr, join = nullptr;
 };
+struct ThreadSplitStreams {
+    SplitStreams per_dev[64];
+    ~ThreadSplitStreams()
+    {
+        for (auto &ss : per_dev) {
+            if (ss.side)
+                cudaStreamDestroy(ss.side);
+            if (ss.fork)
+                cudaEventDestroy(ss.fork);
+            if (ss.join)
+                cudaEventDestroy(ss.join);
+        }
+    }
+};
 static int split_streams(SplitStreams **out)
 {
-    static SplitStreams per_dev[64];
-    static std::mutex mu;
+    static thread_local ThreadSplitStreams mine;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
         return status(e);
     if (dev < 0 || dev >= 64)
         return LBM_ERR_DEVICE;
-    std::lock_guard<std::mutex> lock(mu);
-    SplitStreams &ss = per_dev[dev];
+    SplitStreams &ss = mine.per_dev[dev];
     if (!ss.side) {
-        if ((e = cudaStreamCreateWithFlags(&ss.side, cudaStreamNonBlocking)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming)) != cudaSuccess ||
-            (e = cudaEventCreateWithFlags(&ss.join, cudaEventDisableTiming)) != cudaSuccess)
+        SplitStreams n;
+        if ((e = cudaStreamCreateWithFlags(&n.side, cudaStreamNonBlocking)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&n.fork, cudaEventDisableTiming)) != cudaSuccess ||
+            (e = cudaEventCreateWithFlags(&n.join, cudaEventDisableTiming)) != cudaSuccess) {
+            if (n.side)
+                cudaStreamDestroy(n.side);
+            if (n.fork)
+                cudaEventDestroy(n.fork);
             return status(e);
+        }
+        ss = n;
     }
     *out = &ss;
     return LBM_OK;

@@ -36,10 +36,10 @@ constexpr int kRedThreads = 256;
 
 static int elem_bytes(int storage)
 {
-    return storage == LBM_STORE_F32 ? 4 : 2;
+    return storage == LBM_STORE_F64 ? 8 : (storage == LBM_STORE_F32 ? 4 : 2);
 }
 
-template <class St> __device__ __forceinline__ float ld(const void *f, long long i, int q)
+template <class St> __device__ __forceinline__ typename St::R ld(const void *f, long long i, int q)
 {
     return St::load(reinterpret_cast<const typename St::T *>(f)[i], q);
 }
@@ -47,15 +47,17 @@ template <class St> __device__ __forceinline__ float ld(const void *f, long long
 template <class St>
 __global__ void equilibrium_kernel(void *f, const float *rho, const float *ux, const float *uy, long long N)
 {
+    using R = typename St::R;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < N; i += (long long)gridDim.x * blockDim.x) {
-        const float r = rho ? rho[i] : 1.0f;
-        const float u = ux ? ux[i] : 0.0f;
-        const float v = uy ? uy[i] : 0.0f;
-        const float usq = u * u + v * v;
+        const R r = rho ? rho[i] : 1.0f;
+        const R u = ux ? ux[i] : 0.0f;
+        const R v = uy ? uy[i] : 0.0f;
+        const R usq = u * u + v * v;
 #pragma unroll
         for (int q = 0; q < 9; ++q) {
-            const float cu = (float)cx(q) * u + (float)cy(q) * v;
-            const float feq = wgt(q) * r * (1.0f + 3.0f * cu + 4.5f * cu * cu - 1.5f * usq);
+            const R cu = (R)cx(q) * u + (R)cy(q) * v;
+            const R w = q == 0 ? R(4) / R(9) : (q <= 4 ? R(1) / R(9) : R(1) / R(36));
+            const R feq = w * r * (R(1) + R(3) * cu + R(4.5) * cu * cu - R(1.5) * usq);
             reinterpret_cast<typename St::T *>(f)[q * N + i] = St::store(feq, q);
         }
     }
@@ -65,7 +67,7 @@ template <class Si, class So> __global__ void convert_kernel(const void *src, vo
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n9; i += (long long)gridDim.x * blockDim.x) {
         const int q = (int)(i / N);
-        const float v = Si::load(reinterpret_cast<const typename Si::T *>(src)[i], q);
+        const auto v = Si::load(reinterpret_cast<const typename Si::T *>(src)[i], q);
         reinterpret_cast<typename So::T *>(dst)[i] = So::store(v, q);
     }
 }
@@ -103,7 +105,7 @@ __global__ void __launch_bounds__(kRedThreads) diag_partial_kernel(const void *f
     for (long long i = blockIdx.x * (long long)kRedThreads + threadIdx.x; i < N; i += (long long)gridDim.x * kRedThreads) {
         if (mask[i])
             continue;
-        float fl[9];
+        typename St::R fl[9];
 #pragma unroll
         for (int q = 0; q < 9; ++q)
             fl[q] = ld<St>(f, q * N + i, q);
@@ -168,6 +170,8 @@ template <class F> static int by_storage(int storage, F &&fn)
         return fn(StoreF16Dev{});
     case LBM_STORE_BF16DEV:
         return fn(StoreBF16Dev{});
+    case LBM_STORE_F64:
+        return fn(StoreF64{});
     default:
         return LBM_ERR_ARG;
     }
@@ -186,7 +190,7 @@ static int variant_of(const lbm_params &p)
     else if (p.collision == LBM_COLL_MRT && p.closure == LBM_CLOSURE_MLP && !p.ref_clamps && p.u_lid == 0.0f &&
              p.mlp != nullptr)
         return VAR_MRT_MLP;
-    if (p.storage != LBM_STORE_F32 && (v == VAR_MRT_LID || v == VAR_BGK))
+    if ((p.storage == LBM_STORE_F16DEV || p.storage == LBM_STORE_BF16DEV) && (v == VAR_MRT_LID || v == VAR_BGK))
         v = -1;
     return v;
 }
@@ -197,7 +201,7 @@ static int validate(const lbm_params *p)
         return LBM_ERR_ARG;
     if ((long long)p->W * p->H * 9 > (1ll << 40))
         return LBM_ERR_ARG;
-    if (p->storage < LBM_STORE_F32 || p->storage > LBM_STORE_BF16DEV)
+    if (p->storage < LBM_STORE_F32 || p->storage > LBM_STORE_F64)
         return LBM_ERR_ARG;
     if (p->collision != LBM_COLL_BGK && p->collision != LBM_COLL_MRT)
         return LBM_ERR_ARG;
@@ -217,6 +221,8 @@ static int validate(const lbm_params *p)
     if (y != LBM_BC_WALL && y != LBM_BC_PERIODIC)
         return LBM_ERR_ARG;
     if (variant_of(*p) < 0)
+        return LBM_ERR_UNSUPPORTED;
+    if (p->storage == LBM_STORE_F64 && p->closure == LBM_CLOSURE_MLP)
         return LBM_ERR_UNSUPPORTED;
     return LBM_OK;
 }
@@ -275,6 +281,8 @@ struct InplaceParams {
     Phys k;
 };
 int inplace_step(int variant, int storage, const InplaceParams &p, bool local, cudaStream_t s);
+int general_step_f64(const lbm_params &lp, const void *src, void *dst, const uint8_t *mask, float *ux, float *uy,
+                     float *rho, cudaStream_t s);
 
 } // namespace lbm
 
@@ -363,9 +371,12 @@ int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *
 namespace lbm {
 
 // One launch of t steps from src to dst (u, v, rho written when non-null).
+// FP64 storage has one step per launch (lbm_run passes t = 1).
 static int run_launch(lbm_handle *h, void *src, void *dst, const uint8_t *mask, int t, float *ux, float *uy,
                       float *rho, cudaStream_t s)
 {
+    if (h->p.storage == LBM_STORE_F64)
+        return t == 1 ? general_step_f64(h->p, src, dst, mask, ux, uy, rho, s) : LBM_ERR_UNSUPPORTED;
     WaveParams wp;
     memset(&wp, 0, sizeof(wp));
     wp.f_in = src;
@@ -463,6 +474,8 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
         return LBM_ERR_ARG;
     if ((ux || uy || rho) && !(ux && uy && rho))
         return LBM_ERR_ARG;
+    if (h->p.storage == LBM_STORE_F64)
+        T = 1; // the FP64 kernel advances one step per launch
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int launches = 0, done = 0, rc = LBM_OK;
     // Whole pairs of T-step launches before the last launch replay from a CUDA
@@ -524,6 +537,26 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
     return LBM_OK;
 }
 
+int lbm_run_graph_reset(lbm_handle *h)
+{
+    if (!h)
+        return LBM_ERR_ARG;
+    int idle = 0;
+    if (!h->g_busy.compare_exchange_strong(idle, 1))
+        return LBM_ERR_ARG; // an lbm_run on another thread is replaying them
+    cudaError_t e = cudaSuccess;
+    for (auto &g : h->graphs) {
+        if (g.exec) {
+            cudaError_t r = cudaGraphExecDestroy(g.exec);
+            if (r != cudaSuccess && e == cudaSuccess)
+                e = r;
+        }
+        g = PairGraph{};
+    }
+    h->g_busy = 0;
+    return status(e);
+}
+
 int lbm_run_inplace(lbm_handle *h, void *f, const uint8_t *mask, int n_steps, float *ux, float *uy, float *rho,
                     void *stream)
 {
@@ -532,7 +565,7 @@ int lbm_run_inplace(lbm_handle *h, void *f, const uint8_t *mask, int n_steps, fl
         return LBM_ERR_ARG;
     if ((ux || uy || rho) && !(ux && uy && rho))
         return LBM_ERR_ARG;
-    if (h->variant == VAR_MRT_MLP)
+    if (h->variant == VAR_MRT_MLP || h->p.storage == LBM_STORE_F64)
         return LBM_ERR_UNSUPPORTED;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     InplaceParams ip;
@@ -593,12 +626,14 @@ int lbm_periodic_halo_x(void *f, int width, int H, int halo, int storage, void *
 {
     if (!f || H < 1 || halo < 1 || width < 3 * halo)
         return LBM_ERR_ARG;
-    if (storage < LBM_STORE_F32 || storage > LBM_STORE_BF16DEV)
+    if (storage < LBM_STORE_F32 || storage > LBM_STORE_F64)
         return LBM_ERR_ARG;
     const long long n = 9ll * H * 2 * halo;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const long long plane = (long long)width * H;
-    if (storage == LBM_STORE_F32)
+    if (storage == LBM_STORE_F64)
+        periodic_halo_kernel<double><<<grid_for(n), 256, 0, s>>>(static_cast<double *>(f), width, H, halo, plane);
+    else if (storage == LBM_STORE_F32)
         periodic_halo_kernel<float><<<grid_for(n), 256, 0, s>>>(static_cast<float *>(f), width, H, halo, plane);
     else
         periodic_halo_kernel<uint16_t><<<grid_for(n), 256, 0, s>>>(static_cast<uint16_t *>(f), width, H, halo, plane);

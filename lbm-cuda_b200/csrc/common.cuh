@@ -33,12 +33,16 @@ static_assert(opp(1) == 3 && opp(2) == 4 && opp(3) == 1 && opp(4) == 2, "opp");
 static_assert(opp(5) == 7 && opp(6) == 8 && opp(7) == 5 && opp(8) == 6, "opp");
 
 // ---------------------------------------------------------------------------
-// Storage formats of the population planes in HBM.  Arithmetic is always FP32.
-// F16DEV/BF16DEV store the deviation f_q - w_q, which keeps the ~1e-3 relative
-// resolution of a 16-bit float on the small departures from rest.
+// Storage formats of the population planes in HBM.  Arithmetic is FP32 (R) for
+// the kernels of the hot path; F16DEV/BF16DEV store the deviation f_q - w_q,
+// which keeps the ~1e-3 relative resolution of a 16-bit float on the small
+// departures from rest.  F64 (double storage and arithmetic) is the judge format
+// of general_f64.cu and of the format-generic helpers (initialisation,
+// conversion, reductions).
 // ---------------------------------------------------------------------------
 struct StoreF32 {
     using T = float;
+    using R = float;
     static constexpr int kind = LBM_STORE_F32;
     __device__ __forceinline__ static float load(T v, int)
     {
@@ -51,6 +55,7 @@ struct StoreF32 {
 };
 struct StoreF16Dev {
     using T = __half;
+    using R = float;
     static constexpr int kind = LBM_STORE_F16DEV;
     __device__ __forceinline__ static float load(T v, int q)
     {
@@ -63,6 +68,7 @@ struct StoreF16Dev {
 };
 struct StoreBF16Dev {
     using T = __nv_bfloat16;
+    using R = float;
     static constexpr int kind = LBM_STORE_BF16DEV;
     __device__ __forceinline__ static float load(T v, int q)
     {
@@ -71,6 +77,19 @@ struct StoreBF16Dev {
     __device__ __forceinline__ static T store(float f, int q)
     {
         return __float2bfloat16_rn(f - wgt(q));
+    }
+};
+struct StoreF64 {
+    using T = double;
+    using R = double;
+    static constexpr int kind = LBM_STORE_F64;
+    __device__ __forceinline__ static double load(T v, int)
+    {
+        return v;
+    }
+    __device__ __forceinline__ static T store(double f, int)
+    {
+        return f;
     }
 };
 
@@ -120,14 +139,26 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait: gives up after ~2^31 SM cycles (about a second) and returns false.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Give-up limit of every spin-wait on an mbarrier: 2^31 SM cycles, about a
+// second at the B200's clocks.
+constexpr long long kWaitLimitCycles = 1ll << 31;
+
+// Bounded wait: gives up after `limit` SM cycles and returns false (the callers
+// then set the device error word, wait with the same bound for their own copies
+// in flight and return).
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity,
+                                                  long long limit = kWaitLimitCycles)
 {
     if (mbar_try_wait(bar, parity))
         return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity)) {
-        if (clock64() - t0 > (1ll << 31))
+        if (clock64() - t0 > limit)
             return false;
     }
     return true;

@@ -34,8 +34,44 @@ def _ptr(a) -> C.c_void_p:
     raise TypeError(f"cannot take a device pointer of {type(a)!r}")
 
 
-def _stream(stream=None) -> C.c_void_p:
-    """The stream to launch on: explicit, else torch's current stream, else cupy's."""
+def _array_library(arrays) -> str | None:
+    """"torch" or "cupy" for the first device array among `arrays`, else None."""
+    for a in arrays:
+        if a is None or isinstance(a, int):
+            continue
+        if hasattr(a, "data_ptr"):
+            return "torch"
+        data = getattr(a, "data", None)
+        if data is not None and hasattr(data, "ptr"):
+            return "cupy"
+    return None
+
+
+def _torch_stream():
+    try:
+        import torch
+    except ImportError:
+        return None
+    if torch.cuda.is_available() and torch.cuda.is_initialized():
+        return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return None
+
+
+def _cupy_stream():
+    try:
+        import cupy  # type: ignore
+    except ImportError:
+        return None
+    return C.c_void_p(cupy.cuda.get_current_stream().ptr)
+
+
+def _stream(stream=None, *arrays) -> C.c_void_p:
+    """The stream to launch on: explicit; else the current stream of the array
+    library the arguments come from (cupy arrays: cupy's, so that a driver
+    capturing a graph on a cupy stream, lbm_mine2.py:75-81, captures these
+    launches too, even in a process that has also initialised torch; torch
+    tensors: torch's); else torch's current stream when torch is initialised,
+    else cupy's, else the legacy default stream."""
     if stream is not None:
         if isinstance(stream, int):
             return C.c_void_p(stream)
@@ -43,58 +79,52 @@ def _stream(stream=None) -> C.c_void_p:
             if hasattr(stream, attr):
                 return C.c_void_p(getattr(stream, attr))
         raise TypeError(f"unknown stream object {type(stream)!r}")
-    try:
-        import torch
-
-        if torch.cuda.is_available() and torch.cuda.is_initialized():
-            return C.c_void_p(torch.cuda.current_stream().cuda_stream)
-    except ImportError:
-        pass
-    try:  # a cupy driver capturing into a graph uses cupy's current stream
-        import cupy  # type: ignore
-
-        return C.c_void_p(cupy.cuda.get_current_stream().ptr)
-    except ImportError:
-        return C.c_void_p(0)
+    kind = _array_library(arrays)
+    order = (_cupy_stream, _torch_stream) if kind == "cupy" else (_torch_stream, _cupy_stream)
+    for pick in order:
+        s = pick()
+        if s is not None:
+            return s
+    return C.c_void_p(0)
 
 
 def core4_step(mask, f_now, f_out, ux, uy, rho, W, H, tau_inv, u_in, tau_inv_bnd=None, stream=None):
     """lbm_core4_step: one MRT+Smagorinsky step (lbm_core4.cu:7-212)."""
     tb = tau_inv if tau_inv_bnd is None else tau_inv_bnd
     call("lbm_core4_step", _ptr(mask), _ptr(f_now), _ptr(f_out), _ptr(ux), _ptr(uy), _ptr(rho), int(W), int(H),
-         float(tau_inv), float(u_in), float(tb), _stream(stream))
+         float(tau_inv), float(u_in), float(tb), _stream(stream, f_now))
 
 
 def core4_run(mask, f_a, f_b, ux, uy, rho, W, H, tau_inv, u_in, n_steps, T=4, stream=None) -> int:
     """n_steps core4 steps fused T per launch; returns 1 if the result is in f_b, else 0."""
     out = C.c_int(0)
     call("lbm_core4_run", _ptr(mask), _ptr(f_a), _ptr(f_b), _ptr(ux), _ptr(uy), _ptr(rho), int(W), int(H),
-         float(tau_inv), float(u_in), int(n_steps), int(T), _stream(stream), C.byref(out))
+         float(tau_inv), float(u_in), int(n_steps), int(T), _stream(stream, f_a), C.byref(out))
     return out.value
 
 
 def smemaa_step(mask, f_now, f_out, ux, uy, rho, W, H, tau_inv, u_in, T=4, stream=None):
     """lbm_smemaa_step: T BGK steps, shared-memory AA pattern (lbm_core_smemaa.cu:12-547)."""
     call("lbm_smemaa_step", _ptr(mask), _ptr(f_now), _ptr(f_out), _ptr(ux), _ptr(uy), _ptr(rho), int(W), int(H),
-         float(tau_inv), float(u_in), int(T), _stream(stream))
+         float(tau_inv), float(u_in), int(T), _stream(stream, f_now))
 
 
 def blocked_step(mask, f_now, f_out, W, H, tau_inv, u_in, T=6, stream=None):
     """lbm_blocked_step: T BGK steps, end-fused (lbm_core_smemaa_policy.cu:78-425)."""
     call("lbm_blocked_step", _ptr(mask), _ptr(f_now), _ptr(f_out), int(W), int(H), float(tau_inv), float(u_in),
-         int(T), _stream(stream))
+         int(T), _stream(stream, f_now))
 
 
 def macro(f, ux, uy, rho, mask, W, H, u_in, stream=None):
     """lbm_macro: u, v, rho from canonical f (lbm_core_smemaa_policy.cu:431-476)."""
     call("lbm_macro", _ptr(f), _ptr(ux), _ptr(uy), _ptr(rho), _ptr(mask), int(W), int(H), float(u_in),
-         _stream(stream))
+         _stream(stream, f))
 
 
 def visualize(ux, uy, rho, image, mask, W, H, vort_scale, stream=None):
     """lbm_visualize: vorticity colour map into an RGBA8 device buffer (lbm_core4.cu:214-255)."""
     call("lbm_visualize", _ptr(ux), _ptr(uy), _ptr(rho), _ptr(image), _ptr(mask), int(W), int(H),
-         float(vort_scale), _stream(stream))
+         float(vort_scale), _stream(stream, ux))
 
 
 class _Kernel:

@@ -30,6 +30,7 @@ SIGNATURES = {
     "lbm_init_equilibrium": ([_P] * 5 + [_P], _I),
     "lbm_run": ([_P] * 4 + [_I, _I, _P, _P, _P, _P, _IP], _I),
     "lbm_run_inplace": ([_P] * 3 + [_I, _P, _P, _P, _P], _I),
+    "lbm_run_graph_reset": ([_P], _I),
     "lbm_periodic_halo_x": ([_P, _I, _I, _I, _I, _P], _I),
     "lbm_diag_fp64": ([_P] * 4 + [_P], _I),
     "lbm_forces_fp64": ([_P] * 4 + [_P], _I),
@@ -41,6 +42,7 @@ SIGNATURES = {
     "lbm_mlp_pack": ([_P, _P, _F, _P, _P], _I),
     "lbm_convert_state": ([_I, _I, _P, _I, _P, _I, _P], _I),
     "lbm_device_error_flags": ([_IP, _I], _I),
+    "lbm_selftest_wait_timeout": ([C.c_longlong, _I, _P, _P], _I),
     "lbm_batch_create": ([_P, _P, _I, C.POINTER(C.c_void_p)], _I),
     "lbm_batch_destroy": ([_P], _I),
     "lbm_batch_run": ([_P, _I, _I, _P, _IP], _I),

@@ -6,7 +6,7 @@ import ctypes as C
 from . import _lib
 from ._lib import call, lib
 
-STORE_F32, STORE_F16DEV, STORE_BF16DEV = 0, 1, 2
+STORE_F32, STORE_F16DEV, STORE_BF16DEV, STORE_F64 = 0, 1, 2, 3
 COLL_BGK, COLL_MRT = 0, 1
 CLOSURE_NONE, CLOSURE_SMAG, CLOSURE_MLP = 0, 1, 2
 BC_WALL, BC_PERIODIC, BC_ZOUHE, BC_ZOUHE_RAMP, BC_OUTFLOW = 0, 1, 2, 3, 4
@@ -36,12 +36,14 @@ def default_params(W: int, H: int, **overrides) -> Params:
 def _torch_dtype(storage: int):
     import torch
 
-    return {STORE_F32: torch.float32, STORE_F16DEV: torch.float16, STORE_BF16DEV: torch.bfloat16}[storage]
+    return {STORE_F32: torch.float32, STORE_F16DEV: torch.float16, STORE_BF16DEV: torch.bfloat16,
+            STORE_F64: torch.float64}[storage]
 
 
 class Solver:
     """Owns an lbm_handle.  States are torch tensors shaped (9, H, W) in the
-    handle's storage format (float32, or float16/bfloat16 holding f_q - w_q)."""
+    handle's storage format (float32, float16/bfloat16 holding f_q - w_q, or
+    float64: the FP64 judge, one step per launch whatever T)."""
 
     def __init__(self, W: int, H: int, params: Params | None = None, **overrides):
         self.params = params if params is not None else default_params(W, H, **overrides)
@@ -91,6 +93,11 @@ class Solver:
         call("lbm_run", self.handle, _ptr(f_a), _ptr(f_b), _ptr(mask), int(n_steps), int(T), _ptr(ux), _ptr(uy),
              _ptr(rho), _stream(stream), C.byref(out))
         return out.value
+
+    def reset_graphs(self) -> None:
+        """lbm_run_graph_reset: drop the cached launch-pair graphs (call before
+        freeing state buffers whose addresses new buffers may reuse)."""
+        call("lbm_run_graph_reset", self.handle)
 
     def run_checked(self, f_a, f_b, mask, n_steps: int, T: int = 2, check_every: int = 1000, ux=None, uy=None,
                     rho=None, stream=None) -> int:

@@ -54,6 +54,8 @@ def _create(**kw):
     (dict(s_nu=2.0), ERR_ARG),
     (dict(s_nu=0.0), ERR_ARG),
     (dict(storage=7), ERR_ARG),
+    (dict(storage=4), ERR_ARG),
+    (dict(storage=SV.STORE_F64, closure=SV.CLOSURE_MLP, ref_clamps=0, mlp=4096), ERR_UNSUPPORTED),
     (dict(collision=5), ERR_ARG),
     (dict(bc_left=SV.BC_PERIODIC), ERR_ARG),  # periodic on one side only
     (dict(bc_right=SV.BC_ZOUHE), ERR_ARG),  # no inlet on the right
@@ -86,6 +88,10 @@ def test_solver_calls_refuse_bad_arguments(lib):
     assert lib.lbm_mlp_grad(P, P, P, nul, 100, P, P, P, C.c_size_t(4), None) == ERR_ARG  # workspace too small
     assert lib.lbm_mlp_pack(P, P, 1.0, C.c_void_p(4100), None) == ERR_ARG  # unaligned destination
     assert lib.lbm_mlp_pack(P, P, 0.0, P, None) == ERR_ARG
+    # the wait self-test: limit outside 1 .. 2^31, arrive not 0 / 1
+    assert lib.lbm_selftest_wait_timeout(0, 0, None, None) == ERR_ARG
+    assert lib.lbm_selftest_wait_timeout((1 << 31) + 1, 0, None, None) == ERR_ARG
+    assert lib.lbm_selftest_wait_timeout(1000, 2, None, None) == ERR_ARG
 
 
 def test_batch_create_refuses_unsupported_physics(lib):

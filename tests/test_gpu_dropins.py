@@ -261,3 +261,57 @@ def test_split_launch_matches_tile_kernel(kind, T):
     if kind == "smemaa":
         for x, y in zip(ms, mt):
             assert rel_l2(x, y) < 1e-6
+
+
+def test_split_launch_from_two_host_threads():
+    """Two host threads run split AA launches at the same time, each on its own
+    stream and its own state; each result must equal the unsplit tile kernel
+    (LBM_AA_SPLIT=0) on the same inputs.  The split's side stream and fork/join
+    events belong to the calling thread, so neither thread's edge-band kernel can
+    wait on the other's stream."""
+    import os
+    import threading
+
+    W, H, n, T = 2048, 2048, 6, 4
+    cases = []
+    for seed in (31, 32):
+        m = I.random_discs_mask(W, H, 10, 3.0, 12.0, seed)
+        cases.append((m, I.perturbed_state(W, H, seed + 5, amp=0.02)))
+    os.environ["LBM_AA_SPLIT"] = "0"
+    try:
+        want = []
+        for m, f0 in cases:
+            a, b = dev(f0), dev(f0)
+            mac = [torch.zeros((H, W), device="cuda") for _ in range(3)]
+            for _ in range(n):
+                L.smemaa_step(dev(m), a, b, *mac, W, H, 1.7, 0.1, T=T)
+                a, b = b, a
+            want.append(host(a))
+    finally:
+        os.environ.pop("LBM_AA_SPLIT", None)
+
+    got, errors = [None, None], []
+
+    def worker(k):
+        try:
+            st = torch.cuda.Stream()
+            with torch.cuda.stream(st):
+                m, f0 = cases[k]
+                dm, a, b = dev(m), dev(f0), dev(f0)
+                mac = [torch.zeros((H, W), device="cuda") for _ in range(3)]
+                for _ in range(n):
+                    L.smemaa_step(dm, a, b, *mac, W, H, 1.7, 0.1, T=T, stream=st.cuda_stream)
+                    a, b = b, a
+            st.synchronize()
+            got[k] = a.cpu().numpy()
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(2)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    assert not errors, errors
+    for k in range(2):
+        assert rel_l2(got[k], want[k]) < 1e-6

@@ -122,3 +122,28 @@ def test_alternating_buffer_order_keeps_both_graphs():
         assert np.array_equal(host(x), host(p))
     G.close()
     S.close()
+
+
+def test_graph_reset_then_new_buffers():
+    """lbm_run_graph_reset drops the cached graphs: after it, new state buffers
+    (here freed and reallocated, so they may reuse the old addresses) run
+    correctly; the state equals plain launches."""
+    c = CASES["channel_discs"]
+    W, H = c["W"], c["H"]
+    m = dev(_mask("channel_discs", W, H))
+    f0 = I.perturbed_state(W, H, 7, amp=0.02)
+    S = SV.Solver(W, H, **c["kw"])
+    G = SV.Solver(W, H, **c["kw"])
+    x, y = dev(f0), dev(f0)
+    G.run(x, y, m, 40, 2)  # captures a graph for (x, y, m, 2)
+    G.reset_graphs()
+    G.reset_graphs()  # idempotent
+    del x, y
+    torch.cuda.synchronize()
+    x, y = dev(f0), dev(f0)
+    w = G.run(x, y, m, 40, 2)
+    p, q = dev(f0), dev(f0)
+    r = _plain(S, p, q, m, 40, 2, (None, None, None))
+    assert np.array_equal(host(y if w else x), host(r))
+    G.close()
+    S.close()

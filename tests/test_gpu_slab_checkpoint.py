@@ -71,6 +71,39 @@ def test_checkpoint_resume_continues_exactly(tmp_path, storage):
     assert torch.equal((g if w3 else f), straight)
 
 
+def test_checkpoint_resume_of_a_learned_closure_run(tmp_path):
+    """The packed network travels with the checkpoint: a resumed learned-closure
+    run (new process state: weights reloaded from <path>.mlp into a new device
+    buffer) continues bit for bit."""
+    import numpy as np
+
+    from lbm_b200 import closure as CL
+
+    W, H = 192, 80
+    rng = np.random.default_rng(3)
+    net = CL.Mlp(params=CL.init_params(3) + (0.05 * rng.standard_normal(CL.NPARAM)).astype(np.float32),
+                 in_scale=np.full(5, 300.0, np.float32), out_scale=0.002)
+    kw = dict(CHANNEL, ref_clamps=0, closure=SV.CLOSURE_MLP, storage=SV.STORE_F16DEV)
+    m = dev(I.random_discs_mask(W, H, 2, 3.0, 5.0, 8))
+    S = SV.Solver(W, H, mlp=net.packed().data_ptr(), **kw)
+    a = S.new_state()
+    SV.convert_state(dev(I.perturbed_state(W, H, 9, amp=0.02)), SV.STORE_F32, a, SV.STORE_F16DEV)
+    b = a.clone()
+    which = S.run(a, b, m, 10, 2)
+    cur, nxt = (b, a) if which else (a, b)
+    path = str(tmp_path / "mlp_run")
+    CK.save(path, cur, m, storage=SV.STORE_F16DEV, step=10, params=S.params, mlp_packed=net.packed())
+    w2 = S.run(cur, nxt, m, 10, 2)
+    straight = (nxt if w2 else cur).clone()
+    f, mk, hdr = CK.load(path)
+    packed = CK.load_mlp(path)
+    assert packed.data_ptr() != net.packed().data_ptr()
+    S2 = SV.Solver(W, H, params=CK.params_from_header(hdr, mlp=packed))
+    g = f.clone()
+    w3 = S2.run(f, g, mk, 10, 2)
+    assert torch.equal((g if w3 else f), straight)
+
+
 @pytest.mark.parametrize("params", [PERIODIC, CHANNEL], ids=["periodic", "channel"])
 def test_graph_replayed_slab_run_equals_per_launch_run(params):
     """A single-rank slab run replays pairs of (launch, halo copy) from CUDA

@@ -59,6 +59,32 @@ def test_noalloc_matches_diag_two_calls(storage):
 
 
 @pytest.mark.gpu
+def test_noalloc_at_the_size_limit():
+    """Exactly LBM_NOALLOC_MAX_CELLS cells (16384 x 8192, FP16 storage): every
+    partial slot of the fixed array is used and the last block's counter
+    comparison is at its maximum.  Two calls in a row give the same sums (the
+    block counter is back at zero after the first), equal to lbm_diag_fp64."""
+    W, H = 16384, MAX_CELLS // 16384
+    g = torch.Generator(device="cuda").manual_seed(5)
+    f = (0.01 * torch.randn((9, H, W), generator=g, device="cuda")).to(torch.float16)
+    m = (torch.rand((H, W), generator=g, device="cuda") < 0.1).to(torch.uint8)
+    outs = []
+    for _ in range(2):
+        out = torch.full((3,), float("nan"), dtype=torch.float64, device="cuda")
+        assert _noalloc(W, H, SV.STORE_F16DEV, f, m, out) == 0
+        outs.append(out)
+    S = SV.Solver(W, H, storage=SV.STORE_F16DEV)
+    ref = S.diag(f, m)
+    torch.cuda.synchronize()
+    S.close()
+    assert torch.equal(outs[0], outs[1])
+    assert torch.isfinite(outs[0]).all()
+    assert _close(outs[0], ref), (outs[0], ref)
+    del f, m
+    torch.cuda.empty_cache()
+
+
+@pytest.mark.gpu
 def test_noalloc_rejects_domain_above_limit():
     # real buffers of the rejected size, so nothing could be read out of bounds
     W, H = 16384, MAX_CELLS // 16384 + 1
