@@ -208,11 +208,12 @@ def main():
     ap.add_argument("--c4-steps", type=int, default=20000, help="c4: coarse steps")
     ap.add_argument("--c4-epochs", type=int, default=30, help="c4: training epochs")
     ap.add_argument("--c4-nu", type=float, default=5e-4, help="c4: coarse-grid viscosity (the judge runs at 4x)")
+    ap.add_argument("--c4-out", default=None, help="c4: also write the result line to this JSON file")
     ap.add_argument("--inplace", action="store_true",
                     help="one state buffer: lbm_run_inplace (AA pattern, two one-step kernels per pair of steps)")
-    ap.add_argument("--closure", choices=["smag", "mlp"], default="smag",
-                    help="mlp: the learned closure (random-initialised weights of the 5-32-32-1 network, "
-                         "no reference clamps) in place of Smagorinsky")
+    ap.add_argument("--closure", choices=["smag", "mlp", "mlp_silu"], default="smag",
+                    help="mlp: the learned closure (random-initialised weights of the 5-32-32-1 ReLU network, "
+                         "no reference clamps) in place of Smagorinsky; mlp_silu: the same with SiLU")
     args = ap.parse_args()
 
     rank, world, local = dist_env()
@@ -274,11 +275,12 @@ def main():
     mask_np, f0_np = workload()
     mask = torch.from_numpy(mask_np).cuda()
     extra = {}
-    if args.closure == "mlp":
+    if args.closure in ("mlp", "mlp_silu"):
         from lbm_b200.closure import Mlp
 
-        net = Mlp(seed=0, in_scale=np.array([1e3, 1e3, 1e3, 1e3, 1e2], np.float32), out_scale=1e-4)
-        extra = dict(closure=SV.CLOSURE_MLP, mlp=net.packed().data_ptr(), ref_clamps=0)
+        net = Mlp(seed=0, in_scale=np.array([1e3, 1e3, 1e3, 1e3, 1e2], np.float32), out_scale=1e-4,
+                  act="silu" if args.closure == "mlp_silu" else "relu")
+        extra = dict(closure=net.closure, mlp=net.packed().data_ptr(), ref_clamps=0)
     S = Solver(W, H, cs_smag=CS, u_in=U_IN, s_nu=1.0 / TAU, storage=storage, **extra)
     f_a = torch.empty((9, H, W), dtype=S.dtype, device="cuda")
     SV.convert_state(torch.from_numpy(f0_np).cuda(), SV.STORE_F32, f_a, storage)
@@ -643,10 +645,12 @@ def run_c4(args, torch):
     s_e = 1.64, s_eps = 1.54, s_q = 1.9 on both (with all three at 1.1 this flow
     goes unstable on the large grids, in FP64 as in FP32: its peak speed reaches
     Mach 0.38), 20 000 coarse steps, snapshots every 1000.
-    The closure network is trained on the GPU on the filtered snapshots of a
-    judge run from another seed (1); the coarse runs (no closure, Smagorinsky
-    Cs = 0.1, the network; FP32 and FP16 storage) start from the filtered
-    initial state of seed 0 and are compared with that seed's judge."""
+    Two closure networks are trained on the GPU on the filtered snapshots of a
+    judge run from another seed (1): the configured one (SiLU hidden layers,
+    "mlp_silu") and the ReLU one of the fast kernel ("mlp"); the coarse runs (no
+    closure, Smagorinsky Cs = 0.1, both networks; FP32 and FP16 storage) start
+    from the filtered initial state of seed 0 and are compared with that seed's
+    judge."""
     from lbm_b200 import closure as CL
     from lbm_b200 import solver as SV
 
@@ -659,7 +663,10 @@ def run_c4(args, torch):
     t_judge = time.time() - t0
     ns = len(Jt["data"])
     train, test = list(range(1, ns - 2, 2)), list(range(ns - 2, ns))
-    net, mse = CL.a_priori(Jt, train, test, epochs=args.c4_epochs)
+    net, mse = CL.a_priori(Jt, train, test, epochs=args.c4_epochs, act="relu")
+    net_silu, mse_silu = CL.a_priori(Jt, train, test, epochs=args.c4_epochs, act="silu")
+    mse["mlp_silu"] = mse_silu["mlp"]
+    nets = {"mlp": net, "mlp_silu": net_silu}
 
     def clean(v):
         return [None if not np.isfinite(x) else round(float(x), 5) for x in v]
@@ -667,7 +674,7 @@ def run_c4(args, torch):
     res, mlups = {}, {}
     for sname, st in (("f32", SV.STORE_F32), ("f16", SV.STORE_F16DEV)):
         tm = {}
-        r = CL.compare_closures(J, net, cs=0.1, storage=st, timings=tm, spectrum_floor=1e-8)
+        r = CL.compare_closures(J, nets, cs=0.1, storage=st, timings=tm, spectrum_floor=1e-8)
         for name, (l2, spec) in r.items():
             res[f"{name}_{sname}"] = {"velocity_rel_l2": clean(l2), "log_spectrum_l2": clean(spec)}
             t = tm[name]
@@ -682,7 +689,7 @@ def run_c4(args, torch):
     for v in res.values():
         v["first_step_over_1pct"] = first_over(v["velocity_rel_l2"])
     ft = J["fine_timing"]
-    return {"metric": "velocity rel. L2 vs filtered judge", "value": res["mlp_f16"]["velocity_rel_l2"][-1],
+    line = {"metric": "velocity rel. L2 vs filtered judge", "value": res["mlp_silu_f16"]["velocity_rel_l2"][-1],
             "unit": "relative L2", "n_gpus": 1, "steps": steps, "warmup": 0, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32 math; f32 or f16-deviation storage",
             "data": "synthetic",
@@ -696,6 +703,11 @@ def run_c4(args, torch):
             "mlups_periodic_slab_run": mlups,
             "judge_mlups": round(ft["cells"] * ft["steps"] / (ft["ms"] * 1e3), 1),
             "wall_s": {"judges": round(t_judge, 1), "total": round(time.time() - t0, 1)}}
+    line["config"]["value"] = "the configured SiLU network, FP16 storage, at the last snapshot"
+    if args.c4_out:
+        with open(args.c4_out, "w") as fh:
+            json.dump(line, fh, indent=1)
+    return line
 
 
 def run_dropins(args, torch, ref):

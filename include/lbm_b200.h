@@ -112,7 +112,8 @@ int lbm_visualize(const float *ux, const float *uy, const float *rho, uint8_t *i
 #define LBM_COLL_MRT 1
 #define LBM_CLOSURE_NONE 0
 #define LBM_CLOSURE_SMAG 1
-#define LBM_CLOSURE_MLP 2 /* learned eddy viscosity (lbm_params.mlp), see the MLP section below */
+#define LBM_CLOSURE_MLP 2      /* learned eddy viscosity (lbm_params.mlp), ReLU network; see the MLP section */
+#define LBM_CLOSURE_MLP_SILU 3 /* the same with the SiLU network (the configured activation, slower) */
 
 typedef struct lbm_params {
     int W, H;
@@ -126,7 +127,7 @@ typedef struct lbm_params {
     float u_in;    /* Zou-He inlet velocity */
     float u_lid;   /* x velocity of LBM_MASK_MOVING cells */
     int ref_clamps; /* 1: the reference's stabilisers |u| <= 0.4, rho in [0,1.5], f in [0,10] */
-    const void *mlp; /* LBM_CLOSURE_MLP: device pointer to LBM_MLP_PACKED_BYTES from lbm_mlp_pack */
+    const void *mlp; /* LBM_CLOSURE_MLP(_SILU): device pointer to LBM_MLP_PACKED_BYTES from lbm_mlp_pack_act */
 } lbm_params;
 
 typedef struct lbm_handle lbm_handle;
@@ -254,40 +255,58 @@ int lbm_batch_run_separate(lbm_batch *b, int n_steps, int T, void *stream, int *
 int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk);
 
 /* ------------------------------------------------------------------------
- * Learned closure (no reference counterpart): a 5 -> 32 -> 32 -> 1 MLP (ReLU,
- * ReLU, softplus) maps per-cell features to an eddy viscosity nu_t >= 0; the
- * collision then relaxes the stress moments with 1 / (1/s_nu + 3 nu_t) in
- * place of the Smagorinsky rate.  Features of a cell, from its pre-collision
- * populations: the non-equilibrium stress moments n7 = P_xx - P_yy - rho (u^2 -
- * v^2), n8 = P_xy - rho u v and ne = e - rho (3 |u|^2 - 2) (the energy moment),
- * their magnitude sqrt(n7^2 + n8^2), and rho - 1.
+ * Learned closure (no reference counterpart): a 5 -> 32 -> 32 -> 1 MLP (ReLU or
+ * SiLU hidden layers, softplus output) maps per-cell features to an eddy
+ * viscosity nu_t >= 0; the collision then relaxes the stress moments with
+ * 1 / (1/s_nu + 3 nu_t) in place of the Smagorinsky rate.  Features of a cell,
+ * from its pre-collision populations: the non-equilibrium stress moments n7 =
+ * P_xx - P_yy - rho (u^2 - v^2), n8 = P_xy - rho u v and ne = e - rho (3 |u|^2 -
+ * 2) (the energy moment), their magnitude sqrt(n7^2 + n8^2), and rho - 1.
  * Training runs on the GPU through the kernels below (FP32 master weights);
- * inference uses BF16 weights packed by lbm_mlp_pack, on the tensor cores.
+ * inference uses BF16 weights packed by lbm_mlp_pack_act, on the tensor cores.
+ * The closure kind selects the hidden activation of inference:
+ * LBM_CLOSURE_MLP runs a ReLU network, LBM_CLOSURE_MLP_SILU a SiLU one; the
+ * block in lbm_params.mlp must be packed for the same activation (a kernel that
+ * finds another sets bit 1 of the device error word).
  * ------------------------------------------------------------------------ */
 #define LBM_MLP_IN 5
 #define LBM_MLP_HID 32
 #define LBM_MLP_NPARAM (LBM_MLP_HID * LBM_MLP_IN + LBM_MLP_HID + LBM_MLP_HID * LBM_MLP_HID + LBM_MLP_HID + \
                         LBM_MLP_HID + 1) /* W1[32][5], b1[32], W2[32][32], b2[32], w3[32], b3 */
 #define LBM_MLP_PACKED_BYTES 4096
+#define LBM_MLP_ACT_RELU 0 /* relu(a) */
+#define LBM_MLP_ACT_SILU 1 /* silu(a) = a / (1 + exp(-a)) */
 
-/* y[i] = softplus(MLP(x[i])) for n samples x[n][5] (FP32, device). */
+/* y[i] = softplus(MLP(x[i])) for n samples x[n][5] (FP32, device), with the
+ * hidden activation act (LBM_MLP_ACT_*). */
+int lbm_mlp_forward_act(const float *params, int act, const float *x, float *y, int n, void *stream);
+/* lbm_mlp_forward_act with ReLU. */
 int lbm_mlp_forward(const float *params, const float *x, float *y, int n, void *stream);
 /* Bytes of workspace lbm_mlp_grad needs for n samples. */
 size_t lbm_mlp_workspace_bytes(int n);
 /* Gradient of L = (1/n) sum_i w_i (y_i - target_i)^2 (w = NULL: all 1) with
  * respect to the parameters, and L; deterministic (fixed-order reductions). */
+int lbm_mlp_grad_act(const float *params, int act, const float *x, const float *target, const float *weight, int n,
+                     float *grad, float *loss, void *workspace, size_t workspace_bytes, void *stream);
+/* lbm_mlp_grad_act with ReLU. */
 int lbm_mlp_grad(const float *params, const float *x, const float *target, const float *weight, int n, float *grad,
                  float *loss, void *workspace, size_t workspace_bytes, void *stream);
 /* One Adam update of the parameters (step >= 1 for the bias corrections). */
 int lbm_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, float beta1, float beta2,
                  float eps, void *stream);
-/* BF16 inference block for lbm_params.mlp: the features are multiplied by
- * in_scale[5] before the first layer and nu_t = out_scale * softplus(z). */
+/* BF16 inference block for lbm_params.mlp, for the hidden activation act: the
+ * features are multiplied by in_scale[5] before the first layer and nu_t =
+ * out_scale * softplus(z). */
+int lbm_mlp_pack_act(const float *params, int act, const float *in_scale, float out_scale, void *packed,
+                     void *stream);
+/* lbm_mlp_pack_act with ReLU. */
 int lbm_mlp_pack(const float *params, const float *in_scale, float out_scale, void *packed, void *stream);
 
 /* Read (and optionally clear) the device error word of the current device:
  * bit 0 = a bounded device-side wait gave up (the kernel then stopped its work
- * and returned; the launch itself reports success).  Synchronises the device. */
+ * and returned; the launch itself reports success); bit 1 = a learned-closure
+ * block packed for another activation than the closure kind.  Synchronises the
+ * device. */
 int lbm_device_error_flags(int *flags, int clear);
 
 /* Self-test of the give-up path of the bounded device-side waits (no reference

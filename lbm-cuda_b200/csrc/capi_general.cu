@@ -187,9 +187,9 @@ static int variant_of(const lbm_params &p)
         v = (p.u_lid != 0.0f) ? VAR_MRT_LID : VAR_MRT;
     else if (p.collision == LBM_COLL_BGK && p.closure == LBM_CLOSURE_NONE && !p.ref_clamps && p.u_lid == 0.0f)
         v = VAR_BGK;
-    else if (p.collision == LBM_COLL_MRT && p.closure == LBM_CLOSURE_MLP && !p.ref_clamps && p.u_lid == 0.0f &&
-             p.mlp != nullptr)
-        return VAR_MRT_MLP;
+    else if (p.collision == LBM_COLL_MRT && (p.closure == LBM_CLOSURE_MLP || p.closure == LBM_CLOSURE_MLP_SILU) &&
+             !p.ref_clamps && p.u_lid == 0.0f && p.mlp != nullptr)
+        return p.closure == LBM_CLOSURE_MLP ? VAR_MRT_MLP : VAR_MRT_MLP_SILU;
     if ((p.storage == LBM_STORE_F16DEV || p.storage == LBM_STORE_BF16DEV) && (v == VAR_MRT_LID || v == VAR_BGK))
         v = -1;
     return v;
@@ -205,9 +205,10 @@ static int validate(const lbm_params *p)
         return LBM_ERR_ARG;
     if (p->collision != LBM_COLL_BGK && p->collision != LBM_COLL_MRT)
         return LBM_ERR_ARG;
-    if (p->closure != LBM_CLOSURE_NONE && p->closure != LBM_CLOSURE_SMAG && p->closure != LBM_CLOSURE_MLP)
+    const bool mlp = p->closure == LBM_CLOSURE_MLP || p->closure == LBM_CLOSURE_MLP_SILU;
+    if (p->closure != LBM_CLOSURE_NONE && p->closure != LBM_CLOSURE_SMAG && !mlp)
         return LBM_ERR_UNSUPPORTED;
-    if (p->closure == LBM_CLOSURE_MLP && (!p->mlp || (reinterpret_cast<uintptr_t>(p->mlp) & 15u) != 0))
+    if (mlp && (!p->mlp || (reinterpret_cast<uintptr_t>(p->mlp) & 15u) != 0))
         return LBM_ERR_ARG;
     if (!(p->s_nu > 0.0f && p->s_nu < 2.0f))
         return LBM_ERR_ARG;
@@ -222,7 +223,7 @@ static int validate(const lbm_params *p)
         return LBM_ERR_ARG;
     if (variant_of(*p) < 0)
         return LBM_ERR_UNSUPPORTED;
-    if (p->storage == LBM_STORE_F64 && p->closure == LBM_CLOSURE_MLP)
+    if (p->storage == LBM_STORE_F64 && mlp)
         return LBM_ERR_UNSUPPORTED;
     return LBM_OK;
 }
@@ -241,7 +242,7 @@ static Phys make_phys(const lbm_params &p)
     k.u_lid = p.u_lid;
     k.H = p.H;
     k.ramp = p.bc_left == LBM_BC_ZOUHE_RAMP;
-    k.mlp = p.closure == LBM_CLOSURE_MLP ? p.mlp : nullptr;
+    k.mlp = (p.closure == LBM_CLOSURE_MLP || p.closure == LBM_CLOSURE_MLP_SILU) ? p.mlp : nullptr;
     k.flags = (p.collision == LBM_COLL_MRT ? PF_MRT : 0) | (p.closure == LBM_CLOSURE_SMAG ? PF_SMAG : 0) |
               (p.ref_clamps ? (PF_CLAMPU | PF_CLAMPF) : 0);
     return k;
@@ -398,6 +399,8 @@ static int run_launch(lbm_handle *h, void *src, void *dst, const uint8_t *mask, 
     wp.k = h->k;
     if (h->variant == VAR_MRT_MLP)
         return general_launch_mlp(h->p.storage, wp, t, s);
+    if (h->variant == VAR_MRT_MLP_SILU)
+        return general_launch_mlp_silu(h->p.storage, wp, t, s);
     if (h->p.storage == LBM_STORE_F32)
         return general_launch_f32(h->variant, wp, t, s);
     if (h->p.storage == LBM_STORE_F16DEV)
@@ -565,7 +568,7 @@ int lbm_run_inplace(lbm_handle *h, void *f, const uint8_t *mask, int n_steps, fl
         return LBM_ERR_ARG;
     if ((ux || uy || rho) && !(ux && uy && rho))
         return LBM_ERR_ARG;
-    if (h->variant == VAR_MRT_MLP || h->p.storage == LBM_STORE_F64)
+    if (h->variant == VAR_MRT_MLP || h->variant == VAR_MRT_MLP_SILU || h->p.storage == LBM_STORE_F64)
         return LBM_ERR_UNSUPPORTED;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     InplaceParams ip;

@@ -41,11 +41,13 @@ enum : int { PF_MRT = 1, PF_SMAG = 2, PF_CLAMPU = 4, PF_CLAMPF = 8, PF_INLET_SMA
 //   kInletSmag Smagorinsky also at the Zou-He inlet (the reference does not)
 //   kRefOrder  evaluate in the reference's order (drop-ins: rounding closest to the
 //              reference kernels); otherwise the leaner order of collide_bf
+//   kMlpAct    activation of the learned closure's hidden layers (LBM_MLP_ACT_*)
 template <bool kMrt_, bool kSmag_, bool kClampU_, bool kClampF_, bool kInletSmag_, bool kRefOrder_ = false,
-          bool kMlp_ = false>
+          bool kMlp_ = false, int kMlpAct_ = LBM_MLP_ACT_RELU>
 struct Physics {
     static constexpr bool kRuntime = false;
     static constexpr bool kMlp = kMlp_; // learned eddy viscosity in place of Smagorinsky
+    static constexpr int kMlpAct = kMlpAct_;
     static constexpr bool kRefOrder = kRefOrder_;
     static constexpr bool kMrt = kMrt_;
     static constexpr bool kSmag = kSmag_;
@@ -63,11 +65,13 @@ using PhysMrtSmagClamp = Physics<true, true, true, true, false>; // = PhysCore4 
 using PhysMrtSmag = Physics<true, true, false, false, false>;
 using PhysMrt = Physics<true, false, false, false, false>;
 using PhysBgk = Physics<false, false, false, false, false>;
-using PhysMrtMlp = Physics<true, false, false, false, false, false, true>; // MRT + learned closure
+using PhysMrtMlp = Physics<true, false, false, false, false, false, true>; // MRT + learned closure (ReLU)
+using PhysMrtMlpSilu = Physics<true, false, false, false, false, false, true, LBM_MLP_ACT_SILU>; // SiLU network
 // The same choices read from Phys::flags (uniform branches; non-hot paths).
 struct PhysRuntime {
     static constexpr bool kRuntime = true;
     static constexpr bool kMlp = false;
+    static constexpr int kMlpAct = LBM_MLP_ACT_RELU;
     static constexpr bool kRefOrder = true;
     static constexpr bool kMrt = true, kSmag = true, kClampU = true, kClampF = true, kInletSmag = true;
 };

@@ -10,7 +10,15 @@
 namespace lbm {
 
 // General-solver physics variants (lbm_params -> compile-time choices).
-enum : int { VAR_MRT_SMAG_CLAMP = 0, VAR_MRT_SMAG = 1, VAR_MRT = 2, VAR_MRT_LID = 3, VAR_BGK = 4, VAR_MRT_MLP = 5 };
+enum : int {
+    VAR_MRT_SMAG_CLAMP = 0,
+    VAR_MRT_SMAG = 1,
+    VAR_MRT = 2,
+    VAR_MRT_LID = 3,
+    VAR_BGK = 4,
+    VAR_MRT_MLP = 5,      // learned closure, ReLU network
+    VAR_MRT_MLP_SILU = 6, // learned closure, SiLU network
+};
 
 template <class C> int launch_stream(WaveParams p, cudaStream_t s)
 {
@@ -33,20 +41,20 @@ inline bool stream_ok(const WaveParams &p)
 }
 
 // The learned closure runs in the register wavefront kernel only (1 <= T <= 4,
-// TMA-aligned planes, x not periodic).
-template <class St> int launch_step_mlp(const WaveParams &p, int T, cudaStream_t s)
+// TMA-aligned planes, x not periodic).  Ph: PhysMrtMlp or PhysMrtMlpSilu.
+template <class Ph, class St> int launch_step_mlp(const WaveParams &p, int T, cudaStream_t s)
 {
     if (!p.k.mlp || !rwave_ok<typename St::T>(p, T, MODE_GENERAL, true))
         return LBM_ERR_UNSUPPORTED;
     switch (T) {
     case 1:
-        return launch_rwave<RwCfg<1, 1, 1, PhysMrtMlp, St, MODE_GENERAL>>(p, s);
+        return launch_rwave<RwCfg<1, 1, 1, Ph, St, MODE_GENERAL>>(p, s);
     case 2:
-        return launch_rwave<RwCfg<2, 1, 1, PhysMrtMlp, St, MODE_GENERAL>>(p, s);
+        return launch_rwave<RwCfg<2, 1, 1, Ph, St, MODE_GENERAL>>(p, s);
     case 3:
-        return launch_rwave<RwCfg<3, 1, 2, PhysMrtMlp, St, MODE_GENERAL>>(p, s);
+        return launch_rwave<RwCfg<3, 1, 2, Ph, St, MODE_GENERAL>>(p, s);
     case 4:
-        return launch_rwave<RwCfg<4, 1, 2, PhysMrtMlp, St, MODE_GENERAL>>(p, s);
+        return launch_rwave<RwCfg<4, 1, 2, Ph, St, MODE_GENERAL>>(p, s);
     default:
         return LBM_ERR_UNSUPPORTED;
     }
@@ -87,8 +95,9 @@ int launch_step(const WaveParams &p, int T, cudaStream_t s)
 }
 
 // Defined in general_*.cu (one translation unit per storage format; the learned
-// closure in general_mlp.cu).
+// closure in general_mlp.cu (ReLU) and general_mlp_silu.cu).
 int general_launch_mlp(int storage, const WaveParams &p, int T, cudaStream_t s);
+int general_launch_mlp_silu(int storage, const WaveParams &p, int T, cudaStream_t s);
 int general_launch_f32(int variant, const WaveParams &p, int T, cudaStream_t s);
 int general_launch_f16(int variant, const WaveParams &p, int T, cudaStream_t s);
 int general_launch_bf16(int variant, const WaveParams &p, int T, cudaStream_t s);

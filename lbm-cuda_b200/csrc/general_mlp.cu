@@ -1,5 +1,5 @@
 // General-solver kernels with the learned closure (MRT + MLP eddy viscosity),
-// every storage format.
+// ReLU network, every storage format.
 #include "dispatch.cuh"
 
 namespace lbm {
@@ -8,11 +8,11 @@ int general_launch_mlp(int storage, const WaveParams &p, int T, cudaStream_t s)
 {
     switch (storage) {
     case LBM_STORE_F32:
-        return launch_step_mlp<StoreF32>(p, T, s);
+        return launch_step_mlp<PhysMrtMlp, StoreF32>(p, T, s);
     case LBM_STORE_F16DEV:
-        return launch_step_mlp<StoreF16Dev>(p, T, s);
+        return launch_step_mlp<PhysMrtMlp, StoreF16Dev>(p, T, s);
     case LBM_STORE_BF16DEV:
-        return launch_step_mlp<StoreBF16Dev>(p, T, s);
+        return launch_step_mlp<PhysMrtMlp, StoreBF16Dev>(p, T, s);
     default:
         return LBM_ERR_UNSUPPORTED;
     }

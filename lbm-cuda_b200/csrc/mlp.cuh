@@ -1,25 +1,32 @@
-// Learned closure, inference side: the 5 -> 32 -> 32 -> 1 MLP (ReLU, ReLU,
-// softplus) evaluated by one warp for 64 cells (two per lane) on the tensor
-// cores with mma.sync.m16n8k16 (BF16 inputs, FP32 accumulation).
+// Learned closure, inference side: the 5 -> 32 -> 32 -> 1 MLP (ReLU or SiLU
+// hidden layers, softplus output) evaluated by one warp for 64 cells (two per
+// lane) on the tensor cores with mma.sync.m16n8k16 (BF16 inputs, FP32
+// accumulation).
 //
-// Packed weights (MlpPacked, written by lbm_mlp_pack):
+// Packed weights (MlpPacked, written by lbm_mlp_pack_act):
 //   w1[32][16]  first layer, feature k (k < 5) pre-multiplied by in_scale[k],
 //               column 5 holds b1 (the staged features carry a constant 1
 //               there), columns 6..15 zero;
 //   w2[32][32], w3[8][32] (row 0 = w3, rows 1..7 zero), b2[32], b3, out_scale;
-//   all unscaled (BF16 weights; b2, b3 and out_scale FP32).
+//   act: the activation the block was packed for;
+//   BF16 weights; b2, b3 and out_scale FP32.  For SiLU the first two layers
+//   (w1 with its bias column, w2, b2) are packed halved, see below.
 //
 // Per warp: the 64 feature rows are staged as BF16 in 1 KB of shared memory
 // (row c = cell c = 2 lane + n, 8 values: 5 features, 1, 0, 0) and read as A
 // fragments; a layer's accumulators become the next layer's A fragments in
 // registers (the m16n8k16 accumulator layout of two adjacent 8-column tiles is
-// the A layout of one 16-wide k tile).  The activation is ReLU, applied by the
-// FP32 -> BF16x2 conversion that packs the accumulators anyway
-// (cvt.rn.relu.bf16x2.f32), so it costs no instruction; the accumulators start
-// from the bias (or zero) passed as the MMA's C operand.  (A SiLU via
-// tanh.approx.bf16x2 costs a transcendental-unit instruction per pair, which
-// runs at 8 per clock per SM against about 60 for the conversion, and bounded
-// the kernel.)  The output z of a cell is nu_t = out_scale softplus(z).
+// the A layout of one 16-wide k tile).  The activation is applied while the
+// FP32 accumulators are packed to BF16x2:
+//   ReLU: the packing conversion itself (cvt.rn.relu.bf16x2.f32), no extra
+//         instruction;
+//   SiLU: the accumulators hold h = a / 2 (halved weights), and
+//         silu(a) = a sigmoid(a) = h (1 + tanh h): the packing, one
+//         tanh.approx.bf16x2 and one fma.rn.bf16x2 per pair.  The tanh runs on
+//         the transcendental unit (8 per clock per SM against about 60 for the
+//         conversion), which bounds the SiLU kernel.
+// The accumulators start from the bias (or zero) passed as the MMA's C operand.
+// The output z of a cell is nu_t = out_scale softplus(z).
 #pragma once
 
 #include "collide.cuh"
@@ -33,6 +40,7 @@ struct MlpPacked {
     float b2[32];
     float b3;
     float out_scale;
+    int act; // LBM_MLP_ACT_* the block was packed for
 };
 static_assert(sizeof(MlpPacked) <= LBM_MLP_PACKED_BYTES, "packed MLP size");
 
@@ -101,9 +109,25 @@ __device__ __forceinline__ uint32_t relu_bf16x2(float lo, float hi)
     return d;
 }
 
+// The next layer's A fragment from two accumulators: the activation and the
+// packing to BF16x2 (lo in the low half).
+template <int ACT> __device__ __forceinline__ uint32_t act_bf16x2(float lo, float hi)
+{
+    if constexpr (ACT == LBM_MLP_ACT_SILU) {
+        const uint32_t h = pack_bf16x2(lo, hi); // h = a / 2
+        uint32_t t, d;
+        asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(h));
+        asm("fma.rn.bf16x2 %0, %1, %2, %1;" : "=r"(d) : "r"(h), "r"(t)); // h tanh h + h
+        return d;
+    } else {
+        return relu_bf16x2(lo, hi);
+    }
+}
+
 // Eddy viscosity of the lane's two cells from their features x[n][5].  Warp-
 // collective: every lane of the warp calls it together.  stage: 64 x 8 BF16
 // (1 KB) and zbuf: 64 floats of this warp's shared memory.
+template <int ACT>
 __device__ __forceinline__ void mlp_nu_t(const MlpFrag &F, const float (&x)[2][5], __nv_bfloat16 *stage, float *zbuf,
                                          int lane, float (&nu)[2])
 {
@@ -132,14 +156,14 @@ __device__ __forceinline__ void mlp_nu_t(const MlpFrag &F, const float (&x)[2][5
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt)
             mma_bf16(h1[nt], a, F.b1[nt][0], F.b1[nt][1], 0.0f, 0.0f, 0.0f, 0.0f);
-        // ReLU -> layer-2 A fragments (k tile kt = hidden 16 kt .. 16 kt + 15)
+        // activation -> layer-2 A fragments (k tile kt = hidden 16 kt .. 16 kt + 15)
         uint32_t a2[2][4];
 #pragma unroll
         for (int kt = 0; kt < 2; ++kt) {
-            a2[kt][0] = relu_bf16x2(h1[2 * kt][0], h1[2 * kt][1]);
-            a2[kt][1] = relu_bf16x2(h1[2 * kt][2], h1[2 * kt][3]);
-            a2[kt][2] = relu_bf16x2(h1[2 * kt + 1][0], h1[2 * kt + 1][1]);
-            a2[kt][3] = relu_bf16x2(h1[2 * kt + 1][2], h1[2 * kt + 1][3]);
+            a2[kt][0] = act_bf16x2<ACT>(h1[2 * kt][0], h1[2 * kt][1]);
+            a2[kt][1] = act_bf16x2<ACT>(h1[2 * kt][2], h1[2 * kt][3]);
+            a2[kt][2] = act_bf16x2<ACT>(h1[2 * kt + 1][0], h1[2 * kt + 1][1]);
+            a2[kt][3] = act_bf16x2<ACT>(h1[2 * kt + 1][2], h1[2 * kt + 1][3]);
         }
         float h2[4][4];
 #pragma unroll
@@ -151,10 +175,10 @@ __device__ __forceinline__ void mlp_nu_t(const MlpFrag &F, const float (&x)[2][5
         uint32_t a3[2][4];
 #pragma unroll
         for (int kt = 0; kt < 2; ++kt) {
-            a3[kt][0] = relu_bf16x2(h2[2 * kt][0], h2[2 * kt][1]);
-            a3[kt][1] = relu_bf16x2(h2[2 * kt][2], h2[2 * kt][3]);
-            a3[kt][2] = relu_bf16x2(h2[2 * kt + 1][0], h2[2 * kt + 1][1]);
-            a3[kt][3] = relu_bf16x2(h2[2 * kt + 1][2], h2[2 * kt + 1][3]);
+            a3[kt][0] = act_bf16x2<ACT>(h2[2 * kt][0], h2[2 * kt][1]);
+            a3[kt][1] = act_bf16x2<ACT>(h2[2 * kt][2], h2[2 * kt][3]);
+            a3[kt][2] = act_bf16x2<ACT>(h2[2 * kt + 1][0], h2[2 * kt + 1][1]);
+            a3[kt][3] = act_bf16x2<ACT>(h2[2 * kt + 1][2], h2[2 * kt + 1][3]);
         }
         float z0[4], z[4];
         mma_bf16(z0, a3[0], F.b3[0][0], F.b3[0][1], F.b3v, 0.0f, F.b3v, 0.0f);
@@ -250,7 +274,7 @@ __device__ __forceinline__ void collide_pair_mlp(float2 (&f)[9], bool inlet0, bo
     x[0][0] = n7.x, x[0][1] = n8.x, x[0][2] = ne.x, x[0][3] = sqrtf(qq.x), x[0][4] = r.x - 1.0f;
     x[1][0] = n7.y, x[1][1] = n8.y, x[1][2] = ne.y, x[1][3] = sqrtf(qq.y), x[1][4] = r.y - 1.0f;
     float nu[2];
-    mlp_nu_t(F, x, stage, zbuf, lane, nu);
+    mlp_nu_t<Ph::kMlpAct>(F, x, stage, zbuf, lane, nu);
     float2 s = make_float2(__fdividef(1.0f, k.tau0 + 3.0f * nu[0]), __fdividef(1.0f, k.tau0 + 3.0f * nu[1]));
     if (kZh) {
         s.x = inlet0 ? k.s_nu : s.x;

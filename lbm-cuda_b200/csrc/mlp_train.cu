@@ -1,5 +1,6 @@
-// Training kernels of the learned closure: a 5 -> 32 -> 32 -> 1 MLP (ReLU,
-// ReLU, softplus) mapping per-cell features to an eddy viscosity.  FP32 master weights,
+// Training kernels of the learned closure: a 5 -> 32 -> 32 -> 1 MLP (ReLU or
+// SiLU hidden layers, softplus output) mapping per-cell features to an eddy
+// viscosity.  FP32 master weights,
 // one thread per sample; the weight gradient is reduced deterministically
 // (per-block partial sums in a fixed order, then a fixed-order sum over blocks).
 //
@@ -31,12 +32,31 @@ __device__ __forceinline__ float relu_grad(float a)
 {
     return a > 0.0f ? 1.0f : 0.0f;
 }
+// SiLU a sigmoid(a) and its derivative sigmoid(a) (1 + a (1 - sigmoid(a)))
+__device__ __forceinline__ float silu(float a)
+{
+    return a * sigm(a);
+}
+__device__ __forceinline__ float silu_grad(float a)
+{
+    const float s = sigm(a);
+    return s * (1.0f + a * (1.0f - s));
+}
+template <int ACT> __device__ __forceinline__ float act(float a)
+{
+    return ACT == LBM_MLP_ACT_SILU ? silu(a) : relu(a);
+}
+template <int ACT> __device__ __forceinline__ float act_grad(float a)
+{
+    return ACT == LBM_MLP_ACT_SILU ? silu_grad(a) : relu_grad(a);
+}
 __device__ __forceinline__ float softplus(float x)
 {
     return x > 20.0f ? x : log1pf(expf(x));
 }
 
 // Forward of one sample; keeps pre-activations for the backward pass.
+template <int ACT>
 __device__ __forceinline__ float forward1(const float *P, const float *x, float (&a1)[NH], float (&h1)[NH],
                                           float (&a2)[NH], float (&h2)[NH], float &z)
 {
@@ -47,7 +67,7 @@ __device__ __forceinline__ float forward1(const float *P, const float *x, float 
         for (int k = 0; k < NI; ++k)
             s = fmaf(P[OW1 + i * NI + k], x[k], s);
         a1[i] = s;
-        h1[i] = relu(s);
+        h1[i] = act<ACT>(s);
     }
 #pragma unroll
     for (int i = 0; i < NH; ++i) {
@@ -56,7 +76,7 @@ __device__ __forceinline__ float forward1(const float *P, const float *x, float 
         for (int k = 0; k < NH; ++k)
             s = fmaf(P[OW2 + i * NH + k], h1[k], s);
         a2[i] = s;
-        h2[i] = relu(s);
+        h2[i] = act<ACT>(s);
     }
     float s = P[OB3];
 #pragma unroll
@@ -66,6 +86,7 @@ __device__ __forceinline__ float forward1(const float *P, const float *x, float 
     return softplus(s);
 }
 
+template <int ACT>
 __global__ void __launch_bounds__(BT) mlp_forward_kernel(const float *params, const float *x, float *y, int n)
 {
     __shared__ float P[LBM_MLP_NPARAM];
@@ -79,11 +100,12 @@ __global__ void __launch_bounds__(BT) mlp_forward_kernel(const float *params, co
 #pragma unroll
     for (int k = 0; k < NI; ++k)
         xi[k] = x[(long long)s * NI + k];
-    y[s] = forward1(P, xi, a1, h1, a2, h2, z);
+    y[s] = forward1<ACT>(P, xi, a1, h1, a2, h2, z);
 }
 
 // Per-block partial gradient of L = sum_s w_s (y_s - t_s)^2 / sum_s w_s
 // (w_s = 1 when weights are null), and the partial loss sum.
+template <int ACT>
 __global__ void __launch_bounds__(BT) mlp_grad_kernel(const float *params, const float *x, const float *t,
                                                       const float *w, int n, float inv_norm, float *partial)
 {
@@ -102,7 +124,7 @@ __global__ void __launch_bounds__(BT) mlp_grad_kernel(const float *params, const
 #pragma unroll
         for (int k = 0; k < NI; ++k)
             xi[k] = x[(long long)s * NI + k];
-        const float yv = forward1(P, xi, a1, h1, a2, h2, z);
+        const float yv = forward1<ACT>(P, xi, a1, h1, a2, h2, z);
         const float ws = w ? w[s] : 1.0f;
         const float e = yv - t[s];
         loss = ws * e * e * inv_norm;
@@ -115,19 +137,19 @@ __global__ void __launch_bounds__(BT) mlp_grad_kernel(const float *params, const
         for (int i = 0; i < NH; ++i)
             a1[i] = h1[i] = a2[i] = h2[i] = 0.0f;
     }
-    // dL/da2 = dz * w3 * relu'(a2)
+    // dL/da2 = dz * w3 * act'(a2)
     float d2[NH];
 #pragma unroll
     for (int i = 0; i < NH; ++i)
-        d2[i] = dz * P[OW3 + i] * relu_grad(a2[i]);
-    // dL/da1 = (W2^T d2) * relu'(a1)
+        d2[i] = dz * P[OW3 + i] * act_grad<ACT>(a2[i]);
+    // dL/da1 = (W2^T d2) * act'(a1)
 #pragma unroll
     for (int k = 0; k < NH; ++k) {
         float g = 0.0f;
 #pragma unroll
         for (int i = 0; i < NH; ++i)
             g = fmaf(P[OW2 + i * NH + k], d2[i], g);
-        sd1[tid][k] = g * relu_grad(a1[k]);
+        sd1[tid][k] = g * act_grad<ACT>(a1[k]);
     }
 #pragma unroll
     for (int i = 0; i < NH; ++i) {
@@ -225,10 +247,12 @@ __global__ void mlp_adam_kernel(float *params, const float *grad, float *m, floa
 }
 
 // Packing: W1 with in_scale folded in and b1 as column 5, W2, w3 in BF16; b2, b3
-// and out_scale in FP32.
-__global__ void mlp_pack_kernel(const float *P, const float *in_scale, float out_scale, MlpPacked *W)
+// and out_scale in FP32.  For SiLU the first two layers are halved (the
+// inference kernel evaluates silu(a) = h (1 + tanh h) on h = a / 2).
+__global__ void mlp_pack_kernel(const float *P, int act, const float *in_scale, float out_scale, MlpPacked *W)
 {
     const int tid = threadIdx.x;
+    const float hs = act == LBM_MLP_ACT_SILU ? 0.5f : 1.0f;
     for (int i = tid; i < 32 * 16; i += blockDim.x) {
         const int n = i / 16, k = i % 16;
         float v = 0.0f;
@@ -236,18 +260,24 @@ __global__ void mlp_pack_kernel(const float *P, const float *in_scale, float out
             v = P[OW1 + n * NI + k] * in_scale[k];
         else if (k == NI)
             v = P[OB1 + n];
-        W->w1[n][k] = __float2bfloat16_rn(v);
+        W->w1[n][k] = __float2bfloat16_rn(hs * v);
     }
     for (int i = tid; i < 32 * 32; i += blockDim.x)
-        W->w2[i / 32][i % 32] = __float2bfloat16_rn(P[OW2 + i]);
+        W->w2[i / 32][i % 32] = __float2bfloat16_rn(hs * P[OW2 + i]);
     for (int i = tid; i < 8 * 32; i += blockDim.x)
         W->w3[i / 32][i % 32] = __float2bfloat16_rn(i < 32 ? P[OW3 + i] : 0.0f);
     for (int i = tid; i < 32; i += blockDim.x)
-        W->b2[i] = P[OB2 + i];
+        W->b2[i] = hs * P[OB2 + i];
     if (tid == 0) {
         W->b3 = P[OB3];
         W->out_scale = out_scale;
+        W->act = act;
     }
+}
+
+bool act_ok(int act)
+{
+    return act == LBM_MLP_ACT_RELU || act == LBM_MLP_ACT_SILU;
 }
 
 } // namespace
@@ -265,20 +295,29 @@ size_t lbm_mlp_workspace_bytes(int n)
     return nb * (LBM_MLP_NPARAM + 1) * sizeof(float);
 }
 
-int lbm_mlp_forward(const float *params, const float *x, float *y, int n, void *stream)
+int lbm_mlp_forward_act(const float *params, int act, const float *x, float *y, int n, void *stream)
 {
-    if (!params || !x || !y || n < 0)
+    if (!params || !x || !y || n < 0 || !act_ok(act))
         return LBM_ERR_ARG;
     if (n == 0)
         return LBM_OK;
-    mlp_forward_kernel<<<(n + BT - 1) / BT, BT, 0, static_cast<cudaStream_t>(stream)>>>(params, x, y, n);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (act == LBM_MLP_ACT_SILU)
+        mlp_forward_kernel<LBM_MLP_ACT_SILU><<<(n + BT - 1) / BT, BT, 0, s>>>(params, x, y, n);
+    else
+        mlp_forward_kernel<LBM_MLP_ACT_RELU><<<(n + BT - 1) / BT, BT, 0, s>>>(params, x, y, n);
     return status(cudaGetLastError());
 }
 
-int lbm_mlp_grad(const float *params, const float *x, const float *target, const float *weight, int n, float *grad,
-                 float *loss, void *workspace, size_t workspace_bytes, void *stream)
+int lbm_mlp_forward(const float *params, const float *x, float *y, int n, void *stream)
 {
-    if (!params || !x || !target || !grad || !workspace || n < 1)
+    return lbm_mlp_forward_act(params, LBM_MLP_ACT_RELU, x, y, n, stream);
+}
+
+int lbm_mlp_grad_act(const float *params, int act, const float *x, const float *target, const float *weight, int n,
+                     float *grad, float *loss, void *workspace, size_t workspace_bytes, void *stream)
+{
+    if (!params || !x || !target || !grad || !workspace || n < 1 || !act_ok(act))
         return LBM_ERR_ARG;
     if (workspace_bytes < lbm_mlp_workspace_bytes(n))
         return LBM_ERR_ARG;
@@ -287,9 +326,19 @@ int lbm_mlp_grad(const float *params, const float *x, const float *target, const
     float *part = static_cast<float *>(workspace);
     // the loss is normalised by the number of samples (or the sum of the weights,
     // which the caller passes through by scaling them); 1/n here
-    mlp_grad_kernel<<<nb, BT, 0, s>>>(params, x, target, weight, n, 1.0f / (float)n, part);
+    if (act == LBM_MLP_ACT_SILU)
+        mlp_grad_kernel<LBM_MLP_ACT_SILU><<<nb, BT, 0, s>>>(params, x, target, weight, n, 1.0f / (float)n, part);
+    else
+        mlp_grad_kernel<LBM_MLP_ACT_RELU><<<nb, BT, 0, s>>>(params, x, target, weight, n, 1.0f / (float)n, part);
     mlp_reduce_kernel<<<(LBM_MLP_NPARAM + 1 + 255) / 256, 256, 0, s>>>(part, nb, grad, loss);
     return status(cudaGetLastError());
+}
+
+int lbm_mlp_grad(const float *params, const float *x, const float *target, const float *weight, int n, float *grad,
+                 float *loss, void *workspace, size_t workspace_bytes, void *stream)
+{
+    return lbm_mlp_grad_act(params, LBM_MLP_ACT_RELU, x, target, weight, n, grad, loss, workspace, workspace_bytes,
+                            stream);
 }
 
 int lbm_mlp_adam(float *params, const float *grad, float *m, float *v, int step, float lr, float beta1, float beta2,
@@ -304,15 +353,21 @@ int lbm_mlp_adam(float *params, const float *grad, float *m, float *v, int step,
     return status(cudaGetLastError());
 }
 
-int lbm_mlp_pack(const float *params, const float *in_scale, float out_scale, void *packed, void *stream)
+int lbm_mlp_pack_act(const float *params, int act, const float *in_scale, float out_scale, void *packed,
+                     void *stream)
 {
-    if (!params || !in_scale || !packed || !(out_scale > 0.0f))
+    if (!params || !in_scale || !packed || !(out_scale > 0.0f) || !act_ok(act))
         return LBM_ERR_ARG;
     if ((reinterpret_cast<uintptr_t>(packed) & 15u) != 0)
         return LBM_ERR_ARG;
-    mlp_pack_kernel<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(params, in_scale, out_scale,
+    mlp_pack_kernel<<<1, 256, 0, static_cast<cudaStream_t>(stream)>>>(params, act, in_scale, out_scale,
                                                                       static_cast<MlpPacked *>(packed));
     return status(cudaGetLastError());
+}
+
+int lbm_mlp_pack(const float *params, const float *in_scale, float out_scale, void *packed, void *stream)
+{
+    return lbm_mlp_pack_act(params, LBM_MLP_ACT_RELU, in_scale, out_scale, packed, stream);
 }
 
 } // extern "C"

@@ -373,7 +373,10 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
         unsigned char *mb = wbase + 128 + D * C::SLOT + CR * 32 * 8;
         mc.stage = reinterpret_cast<__nv_bfloat16 *>(mb);
         mc.zbuf = reinterpret_cast<float *>(mb + 64 * 8 * 2);
-        mlp_load_frag(static_cast<const MlpPacked *>(p.k.mlp), mc.F, lane);
+        const MlpPacked *W = static_cast<const MlpPacked *>(p.k.mlp);
+        mlp_load_frag(W, mc.F, lane);
+        if (lane == 0 && p.err && W->act != Ph::kMlpAct)
+            atomicOr(p.err, 2); // the block was packed for another activation
     }
 
     const int xs = rx0 + win * C::CW - C::PADL;

@@ -36,6 +36,9 @@ SIGNATURES = {
     "lbm_forces_fp64": ([_P] * 4 + [_P], _I),
     "lbm_diag_fp64_noalloc": ([_I, _I, _I, _P, _P, _P, _P], _I),
     "lbm_mlp_forward": ([_P, _P, _P, _I, _P], _I),
+    "lbm_mlp_forward_act": ([_P, _I, _P, _P, _I, _P], _I),
+    "lbm_mlp_grad_act": ([_P, _I, _P, _P, _P, _I, _P, _P, _P, C.c_size_t, _P], _I),
+    "lbm_mlp_pack_act": ([_P, _I, _P, _F, _P, _P], _I),
     "lbm_mlp_workspace_bytes": ([_I], C.c_size_t),
     "lbm_mlp_grad": ([_P, _P, _P, _P, _I, _P, _P, _P, C.c_size_t, _P], _I),
     "lbm_mlp_adam": ([_P, _P, _P, _P, _I, _F, _F, _F, _F, _P], _I),

@@ -25,7 +25,7 @@ import os
 FORMAT = "lbm-b200-checkpoint"
 VERSION = 1
 MLP_PACKED_BYTES = 4096  # LBM_MLP_PACKED_BYTES
-CLOSURE_MLP = 2          # LBM_CLOSURE_MLP
+CLOSURE_MLPS = (2, 3)    # LBM_CLOSURE_MLP, LBM_CLOSURE_MLP_SILU
 _DTYPES = {0: ("float32", 4), 1: ("float16", 2), 2: ("bfloat16", 2), 3: ("float64", 8)}
 _NP = {4: "<f4", 2: "<i2", 8: "<f8"}
 
@@ -54,7 +54,7 @@ def save(path: str, f, mask, storage: int = 0, step: int = 0, params=None, extra
          mlp_packed=None) -> dict:
     """Writes the state f (torch tensor (9, H, W), any device) and its mask.
 
-    A run with the learned closure (params.closure == LBM_CLOSURE_MLP) must pass
+    A run with the learned closure (LBM_CLOSURE_MLP or _MLP_SILU) must pass
     its packed inference block as `mlp_packed` (the uint8 tensor of
     LBM_MLP_PACKED_BYTES that params.mlp points to, e.g. ``Mlp.packed()``); it is
     written to `<path>.mlp`, since the pointer itself cannot be resumed."""
@@ -65,7 +65,7 @@ def save(path: str, f, mask, storage: int = 0, step: int = 0, params=None, extra
     expect = _torch_dtype(storage)
     if f.dtype != expect:
         raise ValueError(f"state dtype {f.dtype} does not match storage {storage} ({expect})")
-    uses_mlp = params is not None and int(getattr(params, "closure", 0)) == CLOSURE_MLP
+    uses_mlp = params is not None and int(getattr(params, "closure", 0)) in CLOSURE_MLPS
     if uses_mlp and mlp_packed is None:
         raise ValueError("a learned-closure run needs its packed weights: pass mlp_packed=<the lbm_mlp_pack block>")
     if mlp_packed is not None and mlp_packed.numel() * mlp_packed.element_size() != MLP_PACKED_BYTES:
@@ -156,7 +156,7 @@ def params_from_header(hdr, mlp=None):
     p = dict(hdr.get("params") or {})
     p.pop("mlp", None)  # headers never carry a usable pointer
     W, H = p.pop("W", hdr["W"]), p.pop("H", hdr["H"])
-    if int(p.get("closure", 0)) == CLOSURE_MLP:
+    if int(p.get("closure", 0)) in CLOSURE_MLPS:
         if mlp is None:
             raise ValueError("the saved run uses the learned closure: pass mlp=load_mlp(path)")
         p["mlp"] = mlp.data_ptr()

@@ -1,9 +1,11 @@
 """Learned closure: training data from filtered high-resolution runs of this
 solver, training on the GPU with the library's own forward / backward / Adam
-kernels (lbm_mlp_*), and packing for the collision kernel (LBM_CLOSURE_MLP).
+kernels (lbm_mlp_*), and packing for the collision kernel (LBM_CLOSURE_MLP for a
+ReLU network, LBM_CLOSURE_MLP_SILU for a SiLU one).
 
 Model.  nu_t = out_scale * softplus(MLP(in_scale * x)), MLP 5 -> 32 -> 32 -> 1
-with ReLU on both hidden layers; the collision relaxes the stress moments with 1 / (tau0 + 3 nu_t).
+with ReLU or SiLU on both hidden layers; the collision relaxes the stress
+moments with 1 / (tau0 + 3 nu_t).
 The per-cell features x (what the kernel computes from the pre-collision
 populations) are the non-equilibrium stress moments n7 = Pi_xx - Pi_yy - rho
 (u^2 - v^2), n8 = Pi_xy - rho u v, the energy moment ne = e - rho (3 |u|^2 - 2),
@@ -29,6 +31,7 @@ import numpy as np
 from ._lib import call, lib
 
 NI, NH = 5, 32
+ACTS = {"relu": 0, "silu": 1}  # LBM_MLP_ACT_*
 NPARAM = NH * NI + NH + NH * NH + NH + NH + 1
 PACKED_BYTES = 4096
 OW1, OB1 = 0, NH * NI
@@ -55,11 +58,15 @@ def init_params(seed: int = 0) -> np.ndarray:
 
 
 class Mlp:
-    """The closure network with FP32 master parameters on the GPU."""
+    """The closure network with FP32 master parameters on the GPU; act is the
+    hidden activation ("relu" or "silu")."""
 
-    def __init__(self, params=None, in_scale=None, out_scale: float = 1.0, seed: int = 0):
+    def __init__(self, params=None, in_scale=None, out_scale: float = 1.0, seed: int = 0, act: str = "relu"):
         import torch
 
+        if act not in ACTS:
+            raise ValueError(f"unknown activation {act!r}")
+        self.act = act
         p = init_params(seed) if params is None else np.asarray(params, np.float32)
         self.params = torch.from_numpy(p.copy()).cuda()
         self.m = torch.zeros_like(self.params)
@@ -76,7 +83,8 @@ class Mlp:
         from . import _ptr, _stream
 
         y = torch.empty(x.shape[0], dtype=torch.float32, device=x.device)
-        call("lbm_mlp_forward", _ptr(self.params), _ptr(x), _ptr(y), int(x.shape[0]), _stream(None))
+        call("lbm_mlp_forward_act", _ptr(self.params), ACTS[self.act], _ptr(x), _ptr(y), int(x.shape[0]),
+             _stream(None))
         return y
 
     def loss_grad(self, x, t, w=None, workspace=None):
@@ -90,8 +98,8 @@ class Mlp:
             workspace = torch.empty((nbytes + 3) // 4, dtype=torch.float32, device=x.device)
         grad = torch.empty(NPARAM, dtype=torch.float32, device=x.device)
         loss = torch.empty(1, dtype=torch.float32, device=x.device)
-        call("lbm_mlp_grad", _ptr(self.params), _ptr(x), _ptr(t), _ptr(w), n, _ptr(grad), _ptr(loss),
-             _ptr(workspace), C.c_size_t(nbytes), _stream(None))
+        call("lbm_mlp_grad_act", _ptr(self.params), ACTS[self.act], _ptr(x), _ptr(t), _ptr(w), n, _ptr(grad),
+             _ptr(loss), _ptr(workspace), C.c_size_t(nbytes), _stream(None))
         return loss, grad, workspace
 
     def adam(self, grad, lr=1e-3, beta1=0.9, beta2=0.999, eps=1e-8):
@@ -155,17 +163,26 @@ class Mlp:
         if self._packed is None:
             buf = torch.zeros(PACKED_BYTES // 4, dtype=torch.float32, device="cuda")
             sc = torch.from_numpy(self.in_scale).cuda()
-            call("lbm_mlp_pack", _ptr(self.params), _ptr(sc), float(self.out_scale), _ptr(buf), _stream(None))
+            call("lbm_mlp_pack_act", _ptr(self.params), ACTS[self.act], _ptr(sc), float(self.out_scale), _ptr(buf),
+                 _stream(None))
             self._packed = buf
         return self._packed
 
+    @property
+    def closure(self) -> int:
+        """The lbm_params closure kind that runs this network."""
+        from . import solver as SV
+
+        return SV.CLOSURE_MLP_SILU if self.act == "silu" else SV.CLOSURE_MLP
+
     def state(self) -> dict:
         return {"params": self.params.cpu().numpy().tolist(), "in_scale": self.in_scale.tolist(),
-                "out_scale": self.out_scale}
+                "out_scale": self.out_scale, "act": self.act}
 
     @classmethod
     def from_state(cls, st: dict) -> "Mlp":
-        return cls(params=np.array(st["params"], np.float32), in_scale=st["in_scale"], out_scale=st["out_scale"])
+        return cls(params=np.array(st["params"], np.float32), in_scale=st["in_scale"], out_scale=st["out_scale"],
+                   act=st.get("act", "relu"))
 
 
 # ---------------------------------------------------------------------------
@@ -344,13 +361,14 @@ def spectrum_error(snaps, judge, rel_floor: float | None = None):
     return out
 
 
-def compare_closures(J, net: "Mlp", cs: float = 0.1, storage: int = 0, T: int = 2, timings=None,
+def compare_closures(J, net, cs: float = 0.1, storage: int = 0, T: int = 2, timings=None,
                      spectrum_floor: float | None = None):
     """Coarse runs from the filtered initial state with no closure, Smagorinsky
-    (Cs) and the network; relative L2 velocity error and log-spectrum error
-    against the judge per snapshot, for each: {name: (l2, spectrum)}.
-    `timings`, a dict, receives each run's device time ({name: timing});
-    spectrum_floor is spectrum_error's rel_floor."""
+    (Cs) and the network(s); relative L2 velocity error and log-spectrum error
+    against the judge per snapshot, for each: {name: (l2, spectrum)}.  `net` is
+    one Mlp (named "mlp") or a dict {name: Mlp}.  `timings`, a dict, receives
+    each run's device time ({name: timing}); spectrum_floor is
+    spectrum_error's rel_floor."""
     import torch
 
     from . import solver as SV
@@ -359,10 +377,11 @@ def compare_closures(J, net: "Mlp", cs: float = 0.1, storage: int = 0, T: int = 
     mask = torch.zeros((N, N), dtype=torch.uint8)
     se, seps, sq = J.get("rates", (1.1, 1.1, 1.1))
     base = dict(s_nu=1.0 / J["tau0"], ref_clamps=0, storage=storage, s_e=se, s_eps=seps, s_q=sq)
+    nets = net if isinstance(net, dict) else {"mlp": net}
+    runs = [("none", dict(closure=SV.CLOSURE_NONE)), ("smagorinsky", dict(closure=SV.CLOSURE_SMAG, cs_smag=cs))]
+    runs += [(name, dict(closure=n.closure, mlp=n.packed().data_ptr())) for name, n in nets.items()]
     res = {}
-    for name, extra in (("none", dict(closure=SV.CLOSURE_NONE)), ("smagorinsky", dict(closure=SV.CLOSURE_SMAG,
-                                                                                           cs_smag=cs)),
-                        ("mlp", dict(closure=SV.CLOSURE_MLP, mlp=net.packed().data_ptr()))):
+    for name, extra in runs:
         f0 = J["coarse_f0"]
         if storage != SV.STORE_F32:
             f0 = f0 - np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, np.float32)[:, None, None]
@@ -375,15 +394,15 @@ def compare_closures(J, net: "Mlp", cs: float = 0.1, storage: int = 0, T: int = 
     return res
 
 
-def a_priori(J, train_snaps, test_snaps, epochs: int = 120, seed: int = 0, cs: float = 0.1):
-    """Trains a network on the a-priori data of train_snaps and returns it with
-    the mean squared eddy-viscosity error on test_snaps of the network, of
-    Smagorinsky (Cs) and of no closure (nu_t = 0)."""
+def a_priori(J, train_snaps, test_snaps, epochs: int = 120, seed: int = 0, cs: float = 0.1, act: str = "relu"):
+    """Trains a network (hidden activation act) on the a-priori data of
+    train_snaps and returns it with the mean squared eddy-viscosity error on
+    test_snaps of the network, of Smagorinsky (Cs) and of no closure (nu_t = 0)."""
     x = np.concatenate([J["data"][i][0] for i in train_snaps])
     y = np.concatenate([J["data"][i][1] for i in train_snaps])
     xt = np.concatenate([J["data"][i][0] for i in test_snaps])
     yt = np.concatenate([J["data"][i][1] for i in test_snaps])
-    net = Mlp(seed=seed)
+    net = Mlp(seed=seed, act=act)
     net.fit(x, y, epochs=epochs, batch=8192, lr=3e-3, seed=seed)
     pm = net.predict(xt).cpu().numpy()
     ps = smagorinsky_nu(xt, cs, J["tau0"])

@@ -8,7 +8,7 @@ from ._lib import call, lib
 
 STORE_F32, STORE_F16DEV, STORE_BF16DEV, STORE_F64 = 0, 1, 2, 3
 COLL_BGK, COLL_MRT = 0, 1
-CLOSURE_NONE, CLOSURE_SMAG, CLOSURE_MLP = 0, 1, 2
+CLOSURE_NONE, CLOSURE_SMAG, CLOSURE_MLP, CLOSURE_MLP_SILU = 0, 1, 2, 3
 BC_WALL, BC_PERIODIC, BC_ZOUHE, BC_ZOUHE_RAMP, BC_OUTFLOW = 0, 1, 2, 3, 4
 
 

@@ -492,13 +492,14 @@ void visualize(const float *ux, const float *uy, uint8_t *img, const uint8_t *ma
 //   * bc_right outflow: column W-1 is a ghost receiving the post-collision
 //     populations of x = W-2 (lbm_core4.cu:114-116);
 //   * cells that are not updated keep f_out's previous contents.
-// iparams = {W, H, collision(0 BGK, 1 MRT), closure(0 none, 1 Smagorinsky, 2 MLP),
+// iparams = {W, H, collision(0 BGK, 1 MRT), closure(0 none, 1 Smagorinsky, 2 ReLU MLP, 3 SiLU MLP),
 //            bc_left, bc_right, bc_y, ref_clamps}
 // dparams = {s_nu, s_e, s_eps, s_q, cs, u_in, u_lid}
 // BC codes: 0 wall, 1 periodic, 2 Zou-He, 3 Zou-He with ramp, 4 outflow.
 // ---------------------------------------------------------------------------
-// Learned closure (closure code 2): nu_t = out_scale softplus(MLP(in_scale x)),
-// MLP 5 -> 32 -> 32 -> 1 with ReLU, in double precision; x = (n7, n8, ne,
+// Learned closure (closure code 2: ReLU network, 3: SiLU network): nu_t =
+// out_scale softplus(MLP(in_scale x)), MLP 5 -> 32 -> 32 -> 1, in double
+// precision, silu(a) = a / (1 + exp(-a)); x = (n7, n8, ne,
 // |(n7, n8)|, rho - 1) of the pre-collision populations.  Parameters: W1[32][5],
 // b1[32], W2[32][32], b2[32], w3[32], b3 (set by orc_set_mlp).
 struct MlpParams {
@@ -510,7 +511,12 @@ struct MlpParams {
 static MlpParams g_mlp = {{0}, {0}, 1.0, false};
 
 
-template <class S> inline S mlp_rate(const S *f, S r, S u, S v, S tau0)
+inline double mlp_act(double a, bool silu)
+{
+    return silu ? a / (1.0 + std::exp(-a)) : std::max(a, 0.0);
+}
+
+template <class S> inline S mlp_rate(const S *f, S r, S u, S v, S tau0, bool silu)
 {
     const double n7 = double((f[1] - f[2] + f[3] - f[4]) - r * (u * u - v * v));
     const double n8 = double((f[5] - f[6] + f[7] - f[8]) - r * u * v);
@@ -523,13 +529,13 @@ template <class S> inline S mlp_rate(const S *f, S r, S u, S v, S tau0)
         double a = P[160 + i];
         for (int k = 0; k < 5; ++k)
             a += P[i * 5 + k] * x[k] * g_mlp.in_scale[k];
-        h1[i] = std::max(a, 0.0);
+        h1[i] = mlp_act(a, silu);
     }
     for (int i = 0; i < 32; ++i) {
         double a = P[192 + 1024 + i];
         for (int k = 0; k < 32; ++k)
             a += P[192 + i * 32 + k] * h1[k];
-        h2[i] = std::max(a, 0.0);
+        h2[i] = mlp_act(a, silu);
     }
     double z = P[192 + 1024 + 32 + 32];
     for (int k = 0; k < 32; ++k)
@@ -591,8 +597,8 @@ void general_step(const int *ip, const double *dp, const uint8_t *mask, const S 
                 }
                 if (clos == 1)
                     s = smag_rate(f, r, u, v, tau0, cs);
-                else if (clos == 2)
-                    s = mlp_rate(f, r, u, v, tau0);
+                else if (clos == 2 || clos == 3)
+                    s = mlp_rate(f, r, u, v, tau0, clos == 3);
             }
             ux[pid] = u;
             uy[pid] = v;

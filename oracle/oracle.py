@@ -147,7 +147,7 @@ class General:
 
     def __init__(self, W, H, collision="mrt", closure="smag", s_nu=1.8, s_e=1.1, s_eps=1.1, s_q=1.1, cs=0.2,
                  bc_left="zouhe_ramp", bc_right="outflow", bc_y="wall", u_in=0.1, u_lid=0.0, ref_clamps=True):
-        self.ip = np.array([W, H, 1 if collision == "mrt" else 0, {"none": 0, "smag": 1, "mlp": 2}[closure], BC[bc_left],
+        self.ip = np.array([W, H, 1 if collision == "mrt" else 0, {"none": 0, "smag": 1, "mlp": 2, "mlp_silu": 3}[closure], BC[bc_left],
                             BC[bc_right], BC[bc_y], int(bool(ref_clamps))], dtype=np.int32)
         self.dp = np.array([s_nu, s_e, s_eps, s_q, cs, u_in, u_lid], dtype=np.float64)
 

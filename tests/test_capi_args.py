@@ -88,6 +88,10 @@ def test_solver_calls_refuse_bad_arguments(lib):
     assert lib.lbm_mlp_grad(P, P, P, nul, 100, P, P, P, C.c_size_t(4), None) == ERR_ARG  # workspace too small
     assert lib.lbm_mlp_pack(P, P, 1.0, C.c_void_p(4100), None) == ERR_ARG  # unaligned destination
     assert lib.lbm_mlp_pack(P, P, 0.0, P, None) == ERR_ARG
+    # the activation-aware training and packing calls: unknown activation
+    assert lib.lbm_mlp_forward_act(P, 2, P, P, 10, None) == ERR_ARG
+    assert lib.lbm_mlp_grad_act(P, -1, P, P, nul, 10, P, P, P, C.c_size_t(1 << 20), None) == ERR_ARG
+    assert lib.lbm_mlp_pack_act(P, 7, P, 1.0, P, None) == ERR_ARG
     # the wait self-test: limit outside 1 .. 2^31, arrive not 0 / 1
     assert lib.lbm_selftest_wait_timeout(0, 0, None, None) == ERR_ARG
     assert lib.lbm_selftest_wait_timeout((1 << 31) + 1, 0, None, None) == ERR_ARG

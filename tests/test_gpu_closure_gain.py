@@ -9,7 +9,10 @@ Findings asserted here: a priori the network's eddy viscosity is far closer to
 the judge's than Cs = 0.1 Smagorinsky (which over-dissipates at this
 resolution) and no worse than no closure; a posteriori its velocity field
 stays closer to the filtered judge than Smagorinsky's over the first
-snapshots, and its energy spectrum error at the first snapshot is lower."""
+snapshots, and its energy spectrum error at the first snapshot is lower.
+Against no closure there is no gain at this resolution: the judge's subgrid
+viscosity is small, the network learns a weak closure, and its velocity error
+stays within 1 % of the no-closure run's (asserted)."""
 import numpy as np
 import pytest
 
@@ -29,4 +32,5 @@ def test_learned_closure_gain_over_smagorinsky():
     sp = {k: v[1] for k, v in res.items()}
     for i in (1, 2, 3):
         assert l2["mlp"][i] < l2["smagorinsky"][i]
+        assert abs(l2["mlp"][i] / l2["none"][i] - 1.0) < 0.01
     assert sp["mlp"][1] < sp["smagorinsky"][1]

@@ -2,6 +2,7 @@
 differences, the oracle's MLP closure against a constant-viscosity MRT step, and
 the a-priori training targets on analytic fields."""
 import numpy as np
+import pytest
 
 import mlp_oracle as MO
 import oracle as O
@@ -9,20 +10,21 @@ from lbm_b200 import closure as CL
 from lbm_b200 import init as I
 
 
-def test_oracle_gradient_matches_finite_differences():
+@pytest.mark.parametrize("act", ["relu", "silu"])
+def test_oracle_gradient_matches_finite_differences(act):
     rng = np.random.default_rng(0)
     p = CL.init_params(3).astype(np.float64) + 0.05 * rng.standard_normal(MO.NPARAM)
     x = rng.standard_normal((40, 5))
     t = rng.random(40)
     w = rng.random(40) + 0.5
-    _, g = MO.loss_grad(p, x, t, w)
+    _, g = MO.loss_grad(p, x, t, w, act=act)
     idx = rng.choice(MO.NPARAM, 60, replace=False)
     eps = 1e-6
     for i in idx:
         pp, pm = p.copy(), p.copy()
         pp[i] += eps
         pm[i] -= eps
-        fd = (MO.loss_grad(pp, x, t, w)[0] - MO.loss_grad(pm, x, t, w)[0]) / (2 * eps)
+        fd = (MO.loss_grad(pp, x, t, w, act=act)[0] - MO.loss_grad(pm, x, t, w, act=act)[0]) / (2 * eps)
         assert abs(fd - g[i]) <= 1e-6 * max(1.0, abs(fd)) + 1e-9, (i, fd, g[i])
 
 
