@@ -21,7 +21,7 @@ reference does (lbm_mine2.py:106).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--T 1..8] [--storage f32|f16|bf16] [--inplace] [--closure smag|mlp]
-                    [--workload cylinder|batch|dropins|c2|c3|c4]
+                    [--workload cylinder|batch|dropins|c2|c3|c4|like-reference]
 
 --inplace runs the workload in one state buffer (lbm_run_inplace: the AA
 pattern, one pull-push and one local kernel per pair of steps; T = 1 per kernel).
@@ -41,6 +41,12 @@ reports each variant's velocity error per snapshot and MLUPS.
 kernels (lbm_smemaa_step T=4, lbm_blocked_step T=6, lbm_core4_step) and the
 general solver's BGK path at the drivers' 2048 x 512 and at 4096 x 1024; with
 --impl reference, the reference's own kernels on the same inputs.
+
+--workload like-reference runs the reference arm's configuration (the reference's
+constants Cs = 0.20, s = 1.1) through this repository's drop-in entry points with
+u, v, rho written every step (lbm_core4_step), every two steps (lbm_core4_run,
+T = 2 per call) and once per frame, next to the reference kernel in the same
+process.
 
 --impl reference times the reference's own kernel for this path
 (fused_lbmkernel of lbm_core4.cu, MRT + Smagorinsky, one step per launch,
@@ -199,7 +205,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--storage", choices=["f32", "f16", "bf16"], default="f32",
                     help="population storage of the cylinder workload (16-bit: deviations f - w)")
-    ap.add_argument("--workload", choices=["cylinder", "batch", "dropins", "c2", "c3", "c4"], default="cylinder")
+    ap.add_argument("--workload", choices=["cylinder", "batch", "dropins", "c2", "c3", "c4", "like-reference"],
+                    default="cylinder")
     ap.add_argument("--c2-steps", type=int, default=50000, help="c2: physical steps")
     ap.add_argument("--c2-out", default=None, help="c2: CSV file for the drag / lift series")
     ap.add_argument("--c3-marks", default=None, help="c3: comma-separated checkpoints (default 1000,10000,50000)")
@@ -252,11 +259,13 @@ def main():
     from lbm_b200 import solver as SV
     from lbm_b200.solver import Solver
 
-    if args.workload in ("batch", "dropins", "c2", "c3", "c4"):
+    if args.workload in ("batch", "dropins", "c2", "c3", "c4", "like-reference"):
         if args.workload == "batch":
             line = run_batch(args, torch, rank, world, barrier, max_over_ranks)
         elif args.workload == "c2":
             line = run_c2(args, torch)
+        elif args.workload == "like-reference":
+            line = run_like_reference(args, torch)
         elif args.workload == "c3":
             line = run_c3(args, torch)
         elif args.workload == "c4":
@@ -787,6 +796,67 @@ def run_dropins(args, torch, ref):
     if ref:
         line["impl"] = "reference"
     return line
+
+
+def run_like_reference(args, torch):
+    """The reference arm's configuration run through this repository's drop-in
+    entry points, next to the reference kernel in the same process: the bench
+    cylinder with the reference's compile-time constants (Cs = 0.20, s_e = s_eps =
+    s_q = 1.1, lbm_core4.cu:6,123), tau_inv = 1/tau, u_in, the same mask and
+    initial state, and u, v, rho written as often as the reference writes them.
+      core4_step_T1      lbm_core4_step once per step (u, v, rho every step, as the
+                         reference kernel: the like-for-like line);
+      core4_run_T2_each  lbm_core4_run of 2 steps per call (u, v, rho every 2 steps:
+                         the fused launch cannot write the intermediate step's);
+      core4_run_T2_frame lbm_core4_run over the whole frame (u, v, rho once per frame,
+                         like the default line).
+    Each is timed with CUDA events over --steps frames of --frame steps."""
+    import lbm_b200 as L
+
+    ref = run_reference(args, torch)
+    mask_np, f0_np = workload()
+    mask = torch.from_numpy(mask_np).cuda()
+    st = {"a": torch.from_numpy(f0_np).cuda()}
+    st["b"] = st["a"].clone()
+    mac = [torch.zeros((H, W), dtype=torch.float32, device="cuda") for _ in range(3)]
+    ti = 1.0 / TAU
+
+    def step1():
+        for _ in range(args.frame):
+            L.core4_step(mask, st["a"], st["b"], *mac, W, H, ti, U_IN)
+            st["a"], st["b"] = st["b"], st["a"]
+
+    def each2():
+        for _ in range(args.frame // 2):
+            if L.core4_run(mask, st["a"], st["b"], *mac, W, H, ti, U_IN, 2, T=2):
+                st["a"], st["b"] = st["b"], st["a"]
+
+    def frame2():
+        if L.core4_run(mask, st["a"], st["b"], *mac, W, H, ti, U_IN, args.frame, T=2):
+            st["a"], st["b"] = st["b"], st["a"]
+
+    res = {}
+    for name, fn in (("core4_step_T1", step1), ("core4_run_T2_each", each2), ("core4_run_T2_frame", frame2)):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        res[name] = round(W * H * args.steps * args.frame / (e0.elapsed_time(e1) * 1e3), 1)
+    rv = ref.get("value")
+    return {"metric": "MLUPS", "value": res["core4_step_T1"], "unit": "MLUPS", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"cylinder channel {W}x{H}, the reference's constants (Cs=0.20, s=1.1), "
+                                   f"tau_inv=1/{TAU:.5f}, u_in={U_IN}, through the drop-in entry points",
+                       "value": "core4_step_T1: u, v, rho written every step, as the reference"},
+            "mlups": res, "reference_same_process": rv,
+            "ratio_to_reference": {k: (round(v / rv, 3) if rv else None) for k, v in res.items()},
+            "reference_clocks": ref.get("clocks")}
 
 
 def run_reference(args, torch):

@@ -642,10 +642,16 @@ __device__ __forceinline__ void collide_pair(float2 (&f)[9], const Phys &k, floa
         }
     }
     if (Ph::kClampF) {
-        uint32_t mx = 0u;
+        // max of the 18 bit patterns with three-input integer max: 9 operations
+        uint32_t m3[6];
 #pragma unroll
-        for (int q = 0; q < 9; ++q)
-            mx = max(mx, max(fbits(f[q].x), fbits(f[q].y)));
+        for (int k = 0; k < 6; ++k) {
+            const float a = (3 * k) % 2 ? f[(3 * k) / 2].y : f[(3 * k) / 2].x;
+            const float b = (3 * k + 1) % 2 ? f[(3 * k + 1) / 2].y : f[(3 * k + 1) / 2].x;
+            const float c = (3 * k + 2) % 2 ? f[(3 * k + 2) / 2].y : f[(3 * k + 2) / 2].x;
+            m3[k] = __vimax3_u32(fbits(a), fbits(b), fbits(c));
+        }
+        const uint32_t mx = max(__vimax3_u32(m3[0], m3[1], m3[2]), __vimax3_u32(m3[3], m3[4], m3[5]));
         if (mx > fbits(10.0f)) {
 #pragma unroll
             for (int q = 0; q < 9; ++q) {

@@ -60,6 +60,23 @@ template <class Ph, class St> int launch_step_mlp(const WaveParams &p, int T, cu
     }
 }
 
+// Tuning of the T = 2 register wavefront (build-time, for experiments): the
+// resident warps per SM its registers are sized for (0: the RwCfg default), the
+// row lag between its two time levels and its TMA prefetch distance.  Measured
+// on the 4096 x 1024 cylinder (FP32, GLUPS): 16 warps 112, 14 warps 113, 12
+// warps 102; lag 2 at 12 / 14 warps 97 / 65; prefetch 2 rows at 16 / 14 warps
+// 106 / 106, 3 rows at 12 warps 107: the defaults (16 warps, lag 1, one row
+// ahead) are the fastest.
+#ifndef LBM_RW2_MINB
+#define LBM_RW2_MINB 0
+#endif
+#ifndef LBM_RW2_LAG
+#define LBM_RW2_LAG 1
+#endif
+#ifndef LBM_RW2_P
+#define LBM_RW2_P 1 // rows of TMA prefetch ahead of the row being consumed
+#endif
+
 template <class Ph, class St, int MODE, bool LID = false>
 int launch_step(const WaveParams &p, int T, cudaStream_t s)
 {
@@ -67,7 +84,7 @@ int launch_step(const WaveParams &p, int T, cudaStream_t s)
         return launch_stream<StreamCfg<Ph, St, MODE, LID>>(p, s);
     if (rwave_ok<typename St::T>(p, T, MODE)) {
         if (T == 2)
-            return launch_rwave<RwCfg<2, 1, 1, Ph, St, MODE, LID, true>>(p, s);
+            return launch_rwave<RwCfg<2, 1, LBM_RW2_P, Ph, St, MODE, LID, true, LBM_RW2_MINB, LBM_RW2_LAG>>(p, s);
         if (T == 4)
             return launch_rwave<RwCfg<4, 1, 2, Ph, St, MODE, LID, false>>(p, s);
         return launch_rwave<RwCfg<6, 1, 2, Ph, St, MODE, LID, false>>(p, s);

@@ -389,8 +389,10 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
     const int xm = floor_div(xs, 16) * 16;
     const int offf = (xs - xa) + 2 * lane; // element offset of the lane's pair in a ring row
     const int offm = (xs - xm) + 2 * lane; // byte offset of the lane's mask pair
-    // Columns at or next to the domain's left/right ends are always special.
+    // Columns at or next to the domain's left/right ends are always special
+    // (for the whole window).
     const bool colspec = !PRE && (x <= 0 || x + 1 >= p.W - 2);
+    const bool wcolspec = __any_sync(M, colspec);
     const bool core0 = 2 * lane >= C::PADL && 2 * lane < 64 - C::PADL;
     // Window-wide work of the generic body: Zou-He inlet and outlet ghost.
     const bool win_inlet =
@@ -443,6 +445,7 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
         }
 
     uint32_t hist = 0; // bit t-1: the row of level t in this iteration is special
+    uint32_t rhist = 0; // bit d: ring row i - d has a nonzero mask byte in the window
     int s0 = 0, ph = 0; // slot and phase of ring row i
     int abort = 0, i_ab = 0;
     for (int i = 0; i < nrows; ++i) {
@@ -488,24 +491,30 @@ __device__ __forceinline__ void rwave_run(const WaveParams &p, const CUtensorMap
         }
 
         // ---- codes of level 1's row (yk - 1) from mask rows yk-2 .. yk ----
+        // The row is special when the window's columns hold a nonzero mask byte in
+        // one of the three rows (one vote per new row, kept as a bit history), or
+        // it lies at a domain end; the neighbourhood words and codes are built
+        // only then.  (The window's 64 columns cover the neighbourhoods of every
+        // cell whose value is used: columns 1 .. 62 at level 1.)
         {
-            uint32_t mw[3];
-            const unsigned char *mb[3] = {ring + s2 * C::SLOT + C::SLOT_F, ring + s1 * C::SLOT + C::SLOT_F,
-                                          ring + s0 * C::SLOT + C::SLOT_F};
-#pragma unroll
-            for (int d = 0; d < 3; ++d) {
-                const uint32_t own = *reinterpret_cast<const uint16_t *>(mb[d] + offm);
-                const uint32_t lft = __shfl_up_sync(M, own, 1);
-                const uint32_t rgt = __shfl_down_sync(M, own, 1);
-                mw[d] = ((lft >> 8) & 0xffu) | (own << 8) | ((rgt & 0xffu) << 24);
-            }
+            const uint32_t own_new = *reinterpret_cast<const uint16_t *>(ring + s0 * C::SLOT + C::SLOT_F + offm);
+            rhist = (rhist << 1) | (__any_sync(M, own_new != 0u) ? 1u : 0u);
             const int R1 = yk - 1;
             const bool rowspec = !PRE && !pyper && (R1 <= 0 || R1 >= p.H - 1);
-            const bool spec = colspec || rowspec || ((mw[0] | mw[1] | mw[2]) != 0u);
-            const bool wspec = __any_sync(M, spec);
+            const bool wspec = wcolspec || rowspec || (rhist & 7u) != 0u;
             hist = (hist << 1) | (wspec ? 1u : 0u);
             uint2 cc = make_uint2(0u, 0u);
             if (wspec) {
+                uint32_t mw[3];
+                const unsigned char *mb[3] = {ring + s2 * C::SLOT + C::SLOT_F, ring + s1 * C::SLOT + C::SLOT_F,
+                                              ring + s0 * C::SLOT + C::SLOT_F};
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const uint32_t own = *reinterpret_cast<const uint16_t *>(mb[d] + offm);
+                    const uint32_t lft = __shfl_up_sync(M, own, 1);
+                    const uint32_t rgt = __shfl_down_sync(M, own, 1);
+                    mw[d] = ((lft >> 8) & 0xffu) | (own << 8) | ((rgt & 0xffu) << 24);
+                }
                 uint32_t c2[2];
                 codes_from_bytes<PRE ? (int)MODE_GENERAL : C::MODE, C::LID>(mw, oob_cols, x, R1, p.W, p.H,
                                                                             PRE ? (int)LBM_BC_WALL : p.bc_left,
