@@ -167,6 +167,26 @@ int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *
 int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_steps, int T, float *ux, float *uy,
             float *rho, void *stream, int *result_in_b);
 
+/* One launch of T steps from src to dst that writes only the columns [x0, x1)
+ * of dst (x0, x1 even, 0 <= x0 < x1 <= W); every other column of dst keeps its
+ * contents (no counterpart in the reference, whose kernels cover the whole
+ * domain).  The x-slab decomposition computes a rank's edge columns with it
+ * first, sends them while the interior columns compute, then fills its halos.
+ * Needs the register wavefront kernel: T in {2, 4, 6} (1 .. 4 with the learned
+ * closure), TMA-aligned buffers (16-byte bases, W a multiple of 4 elements and
+ * of 16 mask bytes) and x not periodic; otherwise LBM_ERR_UNSUPPORTED. */
+int lbm_run_columns(lbm_handle *h, const void *src, void *dst, const uint8_t *mask, int T, int x0, int x1,
+                    void *stream);
+
+/* Halo columns of a state of `width` columns (9 planes of H rows, elements of
+ * `storage`) to and from one contiguous buffer buf[2][9][H][ncols], in one
+ * launch each (no counterpart in the reference): side 0 holds columns [xl, xl +
+ * ncols), side 1 columns [xr, xr + ncols); a negative xl or xr skips that side
+ * (its part of buf is neither read nor written).  The x-slab decomposition packs
+ * the owned edge columns it sends and unpacks the halo columns it receives. */
+int lbm_halo_pack(const void *f, int width, int H, int storage, int xl, int xr, int ncols, void *buf, void *stream);
+int lbm_halo_unpack(void *f, int width, int H, int storage, int xl, int xr, int ncols, const void *buf, void *stream);
+
 /* Drops lbm_run's cached graphs (no counterpart in the reference).  Returns
  * LBM_ERR_ARG while an lbm_run on another thread is replaying them. */
 int lbm_run_graph_reset(lbm_handle *h);

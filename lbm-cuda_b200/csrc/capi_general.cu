@@ -266,6 +266,31 @@ template <class E> __global__ void periodic_halo_kernel(E *f, int width, int H, 
     }
 }
 
+// Halo columns of both sides of a state of `width` columns into (or from) one
+// contiguous buffer buf[side][q][y][c] (side 0: columns [xl, xl + ncols), side
+// 1: [xr, xr + ncols); a side with a negative start is skipped).  Element type of
+// 2, 4 or 8 bytes.
+template <class E, bool PACK>
+__global__ void halo_copy_kernel(E *f, int width, int H, int xl, int xr, int ncols, E *buf)
+{
+    const long long per_side = 9ll * H * ncols;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < 2 * per_side;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int side = (int)(i / per_side);
+        const int x = side == 0 ? xl : xr;
+        if (x < 0)
+            continue;
+        const long long j = i - side * per_side;
+        const int c = (int)(j % ncols);
+        const long long r = j / ncols; // q * H + y
+        E *cell = f + r * width + x + c;   // plane q, row y: (q * H + y) * width
+        if (PACK)
+            buf[i] = *cell;
+        else
+            *cell = buf[i];
+    }
+}
+
 static int grid_for(long long n)
 {
     long long g = (n + 255) / 256;
@@ -373,11 +398,14 @@ namespace lbm {
 
 // One launch of t steps from src to dst (u, v, rho written when non-null).
 // FP64 storage has one step per launch (lbm_run passes t = 1).
+// With x1 > 0 only the columns [x0, x1) of dst are written (the register
+// wavefront kernel's output rectangle; other kernels cannot restrict their
+// output, so such a launch is LBM_ERR_UNSUPPORTED where they would run).
 static int run_launch(lbm_handle *h, void *src, void *dst, const uint8_t *mask, int t, float *ux, float *uy,
-                      float *rho, cudaStream_t s)
+                      float *rho, cudaStream_t s, int x0 = 0, int x1 = 0)
 {
     if (h->p.storage == LBM_STORE_F64)
-        return t == 1 ? general_step_f64(h->p, src, dst, mask, ux, uy, rho, s) : LBM_ERR_UNSUPPORTED;
+        return (t == 1 && x1 == 0) ? general_step_f64(h->p, src, dst, mask, ux, uy, rho, s) : LBM_ERR_UNSUPPORTED;
     WaveParams wp;
     memset(&wp, 0, sizeof(wp));
     wp.f_in = src;
@@ -397,6 +425,15 @@ static int run_launch(lbm_handle *h, void *src, void *dst, const uint8_t *mask, 
     wp.bc_y = h->p.bc_y;
     wp.use_tma = 1;
     wp.k = h->k;
+    if (x1 > 0) {
+        const bool mlp = h->variant == VAR_MRT_MLP || h->variant == VAR_MRT_MLP_SILU;
+        const bool ok = h->p.storage == LBM_STORE_F32 ? rwave_ok<float>(wp, t, MODE_GENERAL, mlp)
+                                                      : rwave_ok<uint16_t>(wp, t, MODE_GENERAL, mlp);
+        if (!ok || (mlp && t > 4))
+            return LBM_ERR_UNSUPPORTED;
+        wp.rx0 = x0;
+        wp.rx1 = x1;
+    }
     if (h->variant == VAR_MRT_MLP)
         return general_launch_mlp(h->p.storage, wp, t, s);
     if (h->variant == VAR_MRT_MLP_SILU)
@@ -540,6 +577,18 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
     return LBM_OK;
 }
 
+int lbm_run_columns(lbm_handle *h, const void *src, void *dst, const uint8_t *mask, int T, int x0, int x1,
+                    void *stream)
+{
+    NvtxRange nvtx_range("lbm_run_columns");
+    if (!h || !src || !dst || !mask || src == dst || T < 1 || T > 8)
+        return LBM_ERR_ARG;
+    if (x0 < 0 || x1 > h->p.W || x0 >= x1 || ((x0 | x1) & 1))
+        return LBM_ERR_ARG;
+    return run_launch(h, const_cast<void *>(src), dst, mask, T, nullptr, nullptr, nullptr,
+                      static_cast<cudaStream_t>(stream), x0, x1);
+}
+
 int lbm_run_graph_reset(lbm_handle *h)
 {
     if (!h)
@@ -623,6 +672,46 @@ int lbm_forces_fp64(lbm_handle *h, const void *f, const uint8_t *mask, double *d
         final_reduce_kernel<2><<<1, kRedThreads, 0, s>>>(h->partials, kRedBlocks, d_out);
         return status(cudaGetLastError());
     });
+}
+
+} // extern "C"
+
+namespace lbm {
+template <bool PACK>
+static int halo_copy(void *f, int width, int H, int storage, int xl, int xr, int ncols, void *buf, cudaStream_t s)
+{
+    if (!f || !buf || width < 1 || H < 1 || ncols < 1 || (xl < 0 && xr < 0))
+        return LBM_ERR_ARG;
+    if (xl + ncols > width || xr + ncols > width)
+        return LBM_ERR_ARG;
+    if (storage < LBM_STORE_F32 || storage > LBM_STORE_F64)
+        return LBM_ERR_ARG;
+    const long long n = 2ll * 9 * H * ncols;
+    if (storage == LBM_STORE_F64)
+        halo_copy_kernel<double, PACK><<<grid_for(n), 256, 0, s>>>(static_cast<double *>(f), width, H, xl, xr, ncols,
+                                                                   static_cast<double *>(buf));
+    else if (storage == LBM_STORE_F32)
+        halo_copy_kernel<float, PACK><<<grid_for(n), 256, 0, s>>>(static_cast<float *>(f), width, H, xl, xr, ncols,
+                                                                  static_cast<float *>(buf));
+    else
+        halo_copy_kernel<uint16_t, PACK><<<grid_for(n), 256, 0, s>>>(static_cast<uint16_t *>(f), width, H, xl, xr,
+                                                                     ncols, static_cast<uint16_t *>(buf));
+    return status(cudaGetLastError());
+}
+} // namespace lbm
+
+extern "C" {
+
+int lbm_halo_pack(const void *f, int width, int H, int storage, int xl, int xr, int ncols, void *buf, void *stream)
+{
+    return halo_copy<true>(const_cast<void *>(f), width, H, storage, xl, xr, ncols, buf,
+                           static_cast<cudaStream_t>(stream));
+}
+
+int lbm_halo_unpack(void *f, int width, int H, int storage, int xl, int xr, int ncols, const void *buf, void *stream)
+{
+    return halo_copy<false>(f, width, H, storage, xl, xr, ncols, const_cast<void *>(buf),
+                            static_cast<cudaStream_t>(stream));
 }
 
 int lbm_periodic_halo_x(void *f, int width, int H, int halo, int storage, void *stream)

@@ -31,6 +31,9 @@ SIGNATURES = {
     "lbm_run": ([_P] * 4 + [_I, _I, _P, _P, _P, _P, _IP], _I),
     "lbm_run_inplace": ([_P] * 3 + [_I, _P, _P, _P, _P], _I),
     "lbm_run_graph_reset": ([_P], _I),
+    "lbm_run_columns": ([_P] * 4 + [_I, _I, _I, _P], _I),
+    "lbm_halo_pack": ([_P, _I, _I, _I, _I, _I, _I, _P, _P], _I),
+    "lbm_halo_unpack": ([_P, _I, _I, _I, _I, _I, _I, _P, _P], _I),
     "lbm_periodic_halo_x": ([_P, _I, _I, _I, _I, _P], _I),
     "lbm_diag_fp64": ([_P] * 4 + [_P], _I),
     "lbm_forces_fp64": ([_P] * 4 + [_P], _I),

@@ -10,6 +10,15 @@ are confined to the halo.  Then neighbouring ranks exchange their outermost
 owned columns (one send/recv pair per side, torch.distributed: NCCL between
 GPUs, gloo on CPU) and the halos are current again.
 
+With more than one rank the exchange overlaps the launch (`overlap`, on by
+default where the steps can be restricted to a column range): each launch
+first computes the owned edge columns that the neighbours need (h columns per
+side with a neighbour), packs them into one contiguous buffer (one kernel),
+and starts the send/receive pairs; the interior columns compute meanwhile (on a
+second CUDA stream on the GPU); the received columns are then unpacked into
+the halos (one kernel).  The result equals the plain schedule bit for bit:
+every column is computed by the same kernel from the same inputs.
+
 Global mass and momentum are the FP64 sums over the owned columns of every rank
 (one all-reduce of three doubles).  `gather` / `scatter` move the global state
 to and from rank 0 (checkpoints, output).
@@ -68,29 +77,37 @@ class SlabSolver:
 
     `stepper`, when given, is a factory make(width, H, local_params) returning
     step(f_a, f_b, mask, n_steps, T) -> 1 if the result is in f_b, else 0, which
-    advances a local state (torch tensors (9, H, width) and (H, width)); by
-    default the steps run on the GPU through `solver.Solver` built for the local
-    width with the local boundary conditions.  `params` are the global
+    advances a local state (torch tensors (9, H, width) and (H, width)); a step
+    with a `columns(f_a, f_b, mask, T, x0, x1)` attribute (one launch writing
+    only columns [x0, x1) of f_b) enables the overlapped exchange.  By default
+    the steps run on the GPU through `solver.Solver` built for the local width
+    with the local boundary conditions (lbm_run, lbm_run_columns).  `params` are the global
     lbm_params overrides (bc_left, bc_right, bc_y, physics); `group` a
     torch.distributed process group (None: the default group, or a single rank
-    when torch.distributed is not set up).
+    when torch.distributed is not set up); `comm` another object with the
+    torch.distributed calls used here (get_rank, get_world_size, P2POp, isend,
+    irecv, batch_isend_irecv, all_reduce, send, recv, broadcast, barrier,
+    get_global_rank), for a transport of the caller's own.  The GPU kernels want
+    local widths (owned columns plus halos) that are multiples of 16 columns
+    (TMA rows); choose `halo` accordingly.
     """
 
     def __init__(self, W: int, H: int, mask, T: int = 2, halo: int | None = None, group=None, stepper=None,
-                 device=None, **params):
+                 device=None, overlap: bool = True, comm=None, **params):
         import torch
 
         from . import solver as SV
 
-        self.dist = None
+        self.dist = comm
         self.group = group
-        try:
-            import torch.distributed as dist
+        if comm is None:
+            try:
+                import torch.distributed as dist
 
-            if dist.is_available() and dist.is_initialized():
-                self.dist = dist
-        except ImportError:
-            pass
+                if dist.is_available() and dist.is_initialized():
+                    self.dist = dist
+            except ImportError:
+                pass
         self.world = self.dist.get_world_size(group) if self.dist else 1
         self.rank = self.dist.get_rank(group) if self.dist else 0
         self.T = int(T)
@@ -112,6 +129,7 @@ class SlabSolver:
         self.local_params = local
         cols = torch.tensor(lay.global_columns(), dtype=torch.long)
         self.mask = mask[:, cols].contiguous().to(self.device)
+        self._columns = None  # one launch restricted to a column range, or None
         if stepper is None:
             self._solver = SV.Solver(lay.width, self.H, **local)
             self.dtype = self._solver.dtype
@@ -119,13 +137,21 @@ class SlabSolver:
             def stepper(f_a, f_b, m, n, t):
                 return self._solver.run(f_a, f_b, m, n, t)
 
+            def columns(f_a, f_b, m, t, x0, x1):
+                self._solver.run_columns(f_a, f_b, m, t, x0, x1)
+
             self.storage = self._solver.params.storage
+            self._columns = columns
         else:
             self._solver = None
             self.dtype = torch.float32
             self.storage = SV.STORE_F32
             stepper = stepper(lay.width, self.H, local)
+            self._columns = getattr(stepper, "columns", None)
         self.stepper = stepper
+        self.overlap = bool(overlap) and self._columns is not None and self.world > 1
+        self._bufs = None
+        self._side = None
         self.f = None
         self.g = None
         self.steps_done = 0
@@ -137,6 +163,14 @@ class SlabSolver:
 
         cols = torch.tensor(self.lay.global_columns(), dtype=torch.long)
         self.f = f_global[:, :, cols].to(device=self.device, dtype=self.dtype).contiguous()
+        self.g = self.f.clone()
+
+    def set_local_state(self, f_local):
+        """Takes this rank's local state (9, H, width), halos included, as it is
+        (the halos become current after the first launch's exchange)."""
+        if tuple(f_local.shape) != (9, self.H, self.lay.width):
+            raise ValueError(f"local state must be (9, {self.H}, {self.lay.width})")
+        self.f = f_local.to(device=self.device, dtype=self.dtype).contiguous()
         self.g = self.f.clone()
 
     def owned(self):
@@ -199,12 +233,118 @@ class SlabSolver:
         if right is not None:
             f[:, :, lay.left + n:] = recv_r[:, :, :lay.right]
 
+    def _edges(self):
+        """Column ranges of one overlapped launch: (left edge, right edge, interior);
+        an edge is None on a side without a neighbour (its columns are interior)."""
+        lay, h = self.lay, self.halo
+        n = lay.x1 - lay.x0
+        left, right = self._neighbours()
+        el = (lay.left, lay.left + h) if left is not None else None
+        er = (lay.left + n - h, lay.left + n) if right is not None else None
+        i0 = lay.left + (h if el else 0)
+        i1 = lay.left + n - (h if er else 0)
+        return el, er, (i0, i1)
+
+    def _overlap_ok(self, t):
+        if not self.overlap:
+            return False
+        el, er, (i0, i1) = self._edges()
+        if i1 <= i0:
+            return False
+        if self._solver is not None:
+            # the GPU kernel that restricts its output wants even column bounds
+            bounds = [i0, i1] + list(el or ()) + list(er or ())
+            if any(b % 2 for b in bounds):
+                return False
+        return True
+
+    def _launch_overlapped(self, t):
+        """One launch of t steps f -> g with the halo exchange overlapped (see the
+        module docstring); returns False (nothing done) when the column-restricted
+        launch is not available for this configuration."""
+        import torch
+
+        from . import solver as SV
+
+        lay, h = self.lay, self.halo
+        n = lay.x1 - lay.x0
+        left, right = self._neighbours()
+        el, er, (i0, i1) = self._edges()
+        f, g = self.f, self.g
+        gpu = self._solver is not None
+        if self._bufs is None:
+            self._bufs = (f.new_empty((2, 9, self.H, h)), f.new_empty((2, 9, self.H, h)))
+        send, recv = self._bufs
+        if gpu:
+            cur = torch.cuda.current_stream()
+            if self._side is None:
+                self._side = torch.cuda.Stream()
+            start = torch.cuda.Event()
+            start.record(cur)
+        try:
+            for e in (el, er):
+                if e is not None:
+                    self._columns(f, g, self.mask, t, e[0], e[1])
+        except Exception as exc:  # the restricted launch does not apply: plain schedule from now on
+            from ._lib import LbmError
+
+            if isinstance(exc, LbmError) and exc.status == 1002:
+                self.overlap = False
+                return False
+            raise
+        if gpu:
+            SV.halo_pack(g, self.storage, el[0] if el else -1, er[0] if er else -1, h, send)
+            self._side.wait_event(start)
+            with torch.cuda.stream(self._side):
+                self._columns(f, g, self.mask, t, i0, i1)
+        else:
+            if el:
+                send[0].copy_(g[:, :, el[0]:el[1]])
+            if er:
+                send[1].copy_(g[:, :, er[0]:er[1]])
+        dist = self.dist
+        ops = []
+        if left is not None and left == right:
+            # two ranks, periodic: both messages go to the same peer; the first send
+            # pairs with the peer's first receive (its right halo)
+            ops = [dist.P2POp(dist.isend, send[0], self._peer(left), self.group),
+                   dist.P2POp(dist.isend, send[1], self._peer(left), self.group),
+                   dist.P2POp(dist.irecv, recv[1], self._peer(left), self.group),
+                   dist.P2POp(dist.irecv, recv[0], self._peer(left), self.group)]
+        else:
+            if left is not None:
+                ops.append(dist.P2POp(dist.isend, send[0], self._peer(left), self.group))
+                ops.append(dist.P2POp(dist.irecv, recv[0], self._peer(left), self.group))
+            if right is not None:
+                ops.append(dist.P2POp(dist.isend, send[1], self._peer(right), self.group))
+                ops.append(dist.P2POp(dist.irecv, recv[1], self._peer(right), self.group))
+        works = dist.batch_isend_irecv(ops)
+        if not gpu:
+            self._columns(f, g, self.mask, t, i0, i1)  # the interior while the messages travel
+        for w in works:
+            w.wait()  # on the GPU: the current stream waits for the transfers
+        if gpu:
+            SV.halo_unpack(g, self.storage, 0 if left is not None else -1, lay.left + n if right is not None else -1,
+                           h, recv)
+            cur.wait_stream(self._side)
+        else:
+            if left is not None:
+                g[:, :, :lay.left] = recv[0][:, :, h - lay.left:]
+            if right is not None:
+                g[:, :, lay.left + n:] = recv[1][:, :, :lay.right]
+        return True
+
     def _graph_pairs(self, pairs: int):
         """`pairs` x (launch f -> g, halo copy on g, launch g -> f, halo copy on f)."""
         import torch
 
+        # one cached pair per buffer order: a call of an odd number of launches
+        # swaps f and g, so consecutive calls alternate between two keys
         key = (self.f.data_ptr(), self.g.data_ptr(), self.mask.data_ptr(), self.T)
-        if getattr(self, "_graphs_key", None) != key:
+        cache = self.__dict__.setdefault("_graph_cache", {})
+        if key not in cache:
+            if len(cache) >= 2:
+                cache.clear()
             T = self.T
             # first calls set up per-device state outside the capture (scratch copies)
             a, b = self.f.clone(), self.g.clone()
@@ -219,11 +359,11 @@ class SlabSolver:
                     self.stepper(src, dst, self.mask, T, T)
                     self._exchange(dst)
                 graphs.append(gr)
-            self._graphs = graphs
-            self._graphs_key = key
+            cache[key] = graphs
+        graphs = cache[key]
         for _ in range(pairs):
-            self._graphs[0].replay()
-            self._graphs[1].replay()
+            graphs[0].replay()
+            graphs[1].replay()
 
     def _peer(self, r):
         if self.group is None or self.dist is None:
@@ -244,10 +384,13 @@ class SlabSolver:
             done = pairs * 2 * self.T
         while done < n_steps:
             t = min(self.T, n_steps - done)
-            which = self.stepper(self.f, self.g, self.mask, t, t)
-            if which:
+            if self._overlap_ok(t) and self._launch_overlapped(t):
                 self.f, self.g = self.g, self.f
-            self.exchange()
+            else:
+                which = self.stepper(self.f, self.g, self.mask, t, t)
+                if which:
+                    self.f, self.g = self.g, self.f
+                self.exchange()
             done += t
         self.steps_done += n_steps
 

@@ -94,6 +94,13 @@ class Solver:
              _ptr(rho), _stream(stream), C.byref(out))
         return out.value
 
+    def run_columns(self, f_a, f_b, mask, T: int, x0: int, x1: int, stream=None) -> None:
+        """lbm_run_columns: one launch of T steps f_a -> f_b writing only columns [x0, x1) of f_b."""
+        from . import _ptr, _stream
+
+        call("lbm_run_columns", self.handle, _ptr(f_a), _ptr(f_b), _ptr(mask), int(T), int(x0), int(x1),
+             _stream(stream))
+
     def reset_graphs(self) -> None:
         """lbm_run_graph_reset: drop the cached launch-pair graphs (call before
         freeing state buffers whose addresses new buffers may reuse)."""
@@ -156,6 +163,25 @@ def convert_state(src, src_storage: int, dst, dst_storage: int, stream=None) -> 
 
     _, H, W = src.shape
     call("lbm_convert_state", int(W), int(H), _ptr(src), int(src_storage), _ptr(dst), int(dst_storage),
+         _stream(stream))
+
+
+def halo_pack(f, storage: int, xl: int, xr: int, ncols: int, buf, stream=None) -> None:
+    """lbm_halo_pack: columns [xl, xl + ncols) and [xr, xr + ncols) of every plane
+    of f (9, H, width) into buf (2, 9, H, ncols); a negative start skips its side."""
+    from . import _ptr, _stream
+
+    _, H, width = f.shape
+    call("lbm_halo_pack", _ptr(f), int(width), int(H), int(storage), int(xl), int(xr), int(ncols), _ptr(buf),
+         _stream(stream))
+
+
+def halo_unpack(f, storage: int, xl: int, xr: int, ncols: int, buf, stream=None) -> None:
+    """lbm_halo_unpack: the reverse of halo_pack."""
+    from . import _ptr, _stream
+
+    _, H, width = f.shape
+    call("lbm_halo_unpack", _ptr(f), int(width), int(H), int(storage), int(xl), int(xr), int(ncols), _ptr(buf),
          _stream(stream))
 
 

@@ -45,6 +45,34 @@ def oracle_stepper(width, H, local):
     return step
 
 
+class OracleColumnsStepper:
+    """The oracle stepper with a column-restricted launch (enables the overlapped
+    exchange): t steps from f_a computed into scratch copies, then only columns
+    [x0, x1) copied into f_b (f_a unchanged).  `log` records the calls."""
+
+    def __init__(self, width, H, local, log=None):
+        self.G = O.General(width, H, **oracle_kwargs(local))
+        self.log = log
+
+    def __call__(self, fa, fb, m, n, t):
+        if self.log is not None:
+            self.log.append(("full",))
+        a, b, mm = fa.numpy(), fb.numpy(), m.numpy()
+        for _ in range(n):
+            self.G.step(mm, a, b)
+            a, b = b, a
+        return n % 2
+
+    def columns(self, fa, fb, m, t, x0, x1):
+        if self.log is not None:
+            self.log.append(("cols", x0, x1))
+        a, b, mm = fa.numpy().copy(), fb.numpy().copy(), m.numpy()
+        for _ in range(t):
+            self.G.step(mm, a, b)
+            a, b = b, a
+        fb.numpy()[:, :, x0:x1] = a[:, :, x0:x1]
+
+
 def inputs(name, W, H):
     if name == "channel":
         m = I.random_discs_mask(W, H, 2, 2.0, 4.0, 7)
@@ -54,7 +82,7 @@ def inputs(name, W, H):
     return m, I.perturbed_state(W, H, 11, amp=0.02)
 
 
-def _rank_main(rank, world, port, name, W, H, T, n, q):
+def _rank_main(rank, world, port, name, W, H, T, n, q, overlap=False):
     import torch.distributed as dist
 
     from lbm_b200.slab import SlabSolver
@@ -63,7 +91,9 @@ def _rank_main(rank, world, port, name, W, H, T, n, q):
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         m, f0 = inputs(name, W, H)
-        S = SlabSolver(W, H, torch.from_numpy(m), T=T, stepper=oracle_stepper, device="cpu", **CASES[name])
+        step = OracleColumnsStepper if overlap else oracle_stepper
+        S = SlabSolver(W, H, torch.from_numpy(m), T=T, stepper=step, device="cpu", overlap=overlap, **CASES[name])
+        assert S.overlap == overlap
         S.set_state(torch.from_numpy(f0))
         S.run(n)
         d = S.diag()
@@ -80,13 +110,15 @@ def _free_port():
         return s.getsockname()[1]
 
 
+@pytest.mark.parametrize("overlap", [False, True], ids=["plain", "overlapped"])
 @pytest.mark.parametrize("name,world", [("channel", 2), ("channel", 3), ("periodic", 2), ("periodic", 3)])
-def test_slabs_equal_whole_domain(name, world):
+def test_slabs_equal_whole_domain(name, world, overlap):
     W, H, T, n = 48, 20, 2, 7
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_rank_main, args=(r, world, port, name, W, H, T, n, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank_main, args=(r, world, port, name, W, H, T, n, q, overlap))
+             for r in range(world)]
     for p in procs:
         p.start()
     got, d = q.get(timeout=240)
@@ -175,3 +207,71 @@ def test_checkpoint_written_by_two_ranks_resumes_on_three(tmp_path):
     ref, _ = O.General(W, H, **oracle_kwargs(CASES["channel"])).run(m, f0, 10)
     assert steps == 10
     assert np.array_equal(got, ref)
+
+
+def _order_main(rank, world, port, W, H, T, q):
+    import torch.distributed as dist
+
+    from lbm_b200.slab import SlabSolver
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        log = []
+        real = dist.batch_isend_irecv
+
+        class _Logged:
+            def __init__(self, w):
+                self.w = w
+
+            def wait(self):
+                log.append(("wait",))
+                return self.w.wait()
+
+        def logged(ops):
+            log.append(("send", len(ops)))
+            return [_Logged(w) for w in real(ops)]
+
+        dist.batch_isend_irecv = logged
+        m, f0 = inputs("channel", W, H)
+        S = SlabSolver(W, H, torch.from_numpy(m), T=T, device="cpu", overlap=True,
+                       stepper=lambda w, h, loc: OracleColumnsStepper(w, h, loc, log), **CASES["channel"])
+        S.set_state(torch.from_numpy(f0))
+        S.run(2 * T)
+        q.put((rank, S.lay.left, S.lay.x1 - S.lay.x0, log))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_overlapped_schedule_order():
+    """Three ranks, two launches: each launch computes the edge columns the
+    neighbours need, then posts the sends and receives, then computes the
+    interior while they are in flight, and only then waits; no full-domain step
+    runs.  The middle rank has two edges, the end ranks one."""
+    W, H, T, world = 48, 20, 2, 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_order_main, args=(r, world, port, W, H, T, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    logs = {}
+    for _ in range(world):
+        rank, left, n, log = q.get(timeout=240)
+        logs[rank] = (left, n, log)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    for rank, (left, n, log) in logs.items():
+        h = T
+        edges = []
+        if rank > 0:
+            edges.append(("cols", left, left + h))
+        if rank < world - 1:
+            edges.append(("cols", left + n - h, left + n))
+        i0 = left + (h if rank > 0 else 0)
+        i1 = left + n - (h if rank < world - 1 else 0)
+        n_ops = 2 * len(edges)
+        waits = [("wait",)] * n_ops
+        one = edges + [("send", n_ops), ("cols", i0, i1)] + waits
+        assert log == one + one, (rank, log)
