@@ -614,6 +614,18 @@ def run_batch(args, torch, rank, world, barrier, max_over_ranks):
     torch.cuda.synchronize()
     ms_sep = max_over_ranks(e0.elapsed_time(e1))
     mlups_sep = cells * steps_per * max(1, args.steps // 3) * world / (ms_sep * 1e3)
+    # the same with one item height for every size class (the tuned one of the largest)
+    _, rows = B.tiles()
+    B.set_tiles(T, [chunk] * len(rows))
+    B.run(steps_per, T)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        B.run(steps_per, T)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_uni = max_over_ranks(e0.elapsed_time(e1))
+    B.set_tiles(T, rows)
     return {
         "metric": "aggregate MLUPS", "value": round(mlups, 1), "unit": "MLUPS", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
@@ -621,7 +633,10 @@ def run_batch(args, torch, rank, world, barrier, max_over_ranks):
         "data": "synthetic",
         "config": {"workload": "batch of 256 MRT+Smagorinsky channel domains, Nx,Ny~U[64,1024], 1-4 discs r 4-32, "
                                "u_in~U[0.02,0.08], FP16 storage, one launch per T steps for all domains, autotuned",
-                   "cells": cells, "T": T, "rows_per_item": chunk, "physical_steps_per_step": steps_per},
+                   "cells": cells, "T": T, "rows_per_item": chunk, "physical_steps_per_step": steps_per,
+                   "rows_per_item_by_size_class": rows,
+                   "size_classes": "cells < 2^17, < 2^19, larger"},
+        "uniform_rows_mlups": round(cells * steps_per * args.steps * world / (ms_uni * 1e3), 1),
         "separate_launches_mlups": round(mlups_sep, 1),
         "speedup_vs_separate": round(mlups / mlups_sep, 3),
         "gpu_launches": args.steps * ((steps_per + T - 1) // T),

@@ -269,10 +269,25 @@ int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in
 /* The same steps with one ordinary launch per domain (the comparison point). */
 int lbm_batch_run_separate(lbm_batch *b, int n_steps, int T, void *stream, int *result_in_b);
 
-/* Time candidate (T, rows per work item) pairs on the batch and keep the fastest
- * for T = 0.  Advances every domain by an even number of steps per candidate
- * (states end in f_a).  Synchronous. */
+/* Tile shape: a work item is one 64-column window (register wavefront) or one
+ * strip (shared-memory wavefront) of a domain by `rows` rows, with `rows` chosen
+ * per domain size class: class 0 below 2^17 cells, class 1 below 2^19, class 2
+ * the rest.  Rows: 8 .. 32 for the register wavefront, 16 .. 128 otherwise, and
+ * at least 2 T. */
+#define LBM_BATCH_SIZE_CLASSES 3
+
+/* Time candidate configurations on the batch and keep the fastest for T = 0:
+ * for every depth T, one row count for all classes first, then each populated
+ * size class's rows in turn with the others held.  *best_chunk receives the rows
+ * of the largest populated class.  Advances every domain by an even number of
+ * steps per candidate (states end in f_a).  Synchronous. */
 int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk);
+
+/* The configuration T = 0 runs (tuned, or the default before lbm_batch_autotune):
+ * the depth and rows[LBM_BATCH_SIZE_CLASSES]. */
+int lbm_batch_get_tiles(const lbm_batch *b, int *T, int *rows);
+/* Sets that configuration (LBM_ERR_ARG for a depth or row count out of range). */
+int lbm_batch_set_tiles(lbm_batch *b, int T, const int *rows);
 
 /* ------------------------------------------------------------------------
  * Learned closure (no reference counterpart): a 5 -> 32 -> 32 -> 1 MLP (ReLU or

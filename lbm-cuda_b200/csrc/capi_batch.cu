@@ -6,6 +6,13 @@
 // take (domain, strip, row-chunk) items from a device counter and run the
 // shared-memory wavefront tile of wave.cuh.  Launch pairs (ping-pong) are
 // captured once into a CUDA graph and replayed.
+//
+// Tile shape: an item is one window (64 columns, register wavefront) or strip
+// (shared-memory wavefront) of a domain by `rows` rows, and `rows` is chosen per
+// domain size class (LBM_BATCH_SIZE_CLASSES classes by cell count): small
+// domains want short items to spread over the GPU, large ones long items that
+// waste less of their wavefront warm-up.  The autotuner searches the depth T,
+// then the rows of every class in turn.
 #include <stdlib.h>
 #include <string.h>
 
@@ -225,6 +232,37 @@ static int separate_launch(int clamps, int storage, const WaveParams &w, int T, 
 
 using namespace lbm;
 
+namespace lbm {
+// Rows per work item for each domain size class.
+struct Rows {
+    int r[LBM_BATCH_SIZE_CLASSES];
+    bool operator==(const Rows &o) const
+    {
+        for (int c = 0; c < LBM_BATCH_SIZE_CLASSES; ++c)
+            if (r[c] != o.r[c])
+                return false;
+        return true;
+    }
+    bool operator!=(const Rows &o) const
+    {
+        return !(*this == o);
+    }
+};
+inline Rows uniform_rows(int v)
+{
+    Rows x;
+    for (int c = 0; c < LBM_BATCH_SIZE_CLASSES; ++c)
+        x.r[c] = v;
+    return x;
+}
+// Size class of a domain of W x H cells: < 2^17 cells, < 2^19, larger.
+inline int size_class(int W, int H)
+{
+    const long long n = (long long)W * H;
+    return n < (1ll << 17) ? 0 : (n < (1ll << 19) ? 1 : 2);
+}
+} // namespace lbm
+
 struct lbm_batch {
     lbm_params p;
     std::vector<lbm_domain> doms;
@@ -234,20 +272,29 @@ struct lbm_batch {
     int max_items = 0;
     int n_items = 0;
     int *d_counter = nullptr;
-    int cur_T = 0, cur_chunk = 0; // configuration the device item list holds
+    int cur_T = 0;                    // configuration the device item list holds
+    Rows cur_rows = uniform_rows(0);
     std::vector<int4> h_items;
-    int tuned_T = 4, tuned_chunk = 64;
+    int tuned_T = 4;
+    Rows tuned_rows = uniform_rows(64);
+    int class_count[LBM_BATCH_SIZE_CLASSES] = {0};
     bool rw_all = false; // every domain can take the register wavefront
     int cur_engine = 0;  // engine the device item list is for: 0 shared-memory wavefront, 1 register
     int tuned_engine = 0;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int exec_T = 0, exec_chunk = 0;
+    int exec_T = 0;
+    Rows exec_rows = uniform_rows(0);
 };
 
-static int batch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
+static int rows_of(const lbm_batch *b, const Rows &rows, int d)
 {
-    if (b->cur_engine == 0 && b->cur_T == T && b->cur_chunk == chunk)
+    return rows.r[size_class(b->doms[d].W, b->doms[d].H)];
+}
+
+static int batch_items(lbm_batch *b, int T, const Rows &rows, cudaStream_t s)
+{
+    if (b->cur_engine == 0 && b->cur_T == T && b->cur_rows == rows)
         return LBM_OK;
     int cw = 0;
     int rc = with_cfg<CwOp>(b->p.ref_clamps, b->p.storage, T, &cw);
@@ -255,6 +302,7 @@ static int batch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
         return rc;
     b->h_items.clear();
     for (int d = 0; d < (int)b->doms.size(); ++d) {
+        const int chunk = rows_of(b, rows, d);
         const int strips = (b->doms[d].W + cw - 1) / cw;
         const int chunks = (b->doms[d].H + chunk - 1) / chunk;
         for (int by = 0; by < chunks; ++by)
@@ -263,8 +311,8 @@ static int batch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
     }
     if ((int)b->h_items.size() > b->max_items)
         return LBM_ERR_ARG;
-    for (auto &hd : b->hdoms)
-        hd.p.chunk = chunk;
+    for (int d = 0; d < (int)b->hdoms.size(); ++d)
+        b->hdoms[d].p.chunk = rows_of(b, rows, d);
     cudaError_t e = cudaMemcpyAsync(b->d_items, b->h_items.data(), sizeof(int4) * b->h_items.size(),
                                     cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess)
@@ -276,7 +324,7 @@ static int batch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
         return status(e);
     b->n_items = (int)b->h_items.size();
     b->cur_T = T;
-    b->cur_chunk = chunk;
+    b->cur_rows = rows;
     return LBM_OK;
 }
 
@@ -287,9 +335,9 @@ static bool rw_engine(const lbm_batch *b, int T)
 
 // Item list of the register wavefront for (T, chunk): the edge windows of every
 // domain first (half-height items), then all other windows.
-static int rbatch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
+static int rbatch_items(lbm_batch *b, int T, const Rows &rows, cudaStream_t s)
 {
-    if (b->cur_engine == 1 && b->cur_T == T && b->cur_chunk == chunk)
+    if (b->cur_engine == 1 && b->cur_T == T && b->cur_rows == rows)
         return LBM_OK;
     int cw = 0, padl = 0;
     int rc = with_rcfg<RGeomOp>(b->p.ref_clamps, b->p.storage, T, &cw, &padl);
@@ -298,6 +346,7 @@ static int rbatch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
     b->h_items.clear();
     std::vector<int4> mid;
     for (int d = 0; d < (int)b->doms.size(); ++d) {
+        const int chunk = rows_of(b, rows, d);
         const RwItems it = rw_items(b->doms[d].W, b->doms[d].H, cw, padl, chunk);
         for (int i = 0; i < it.n_items; ++i) {
             int win, ya, yb;
@@ -319,25 +368,31 @@ static int rbatch_items(lbm_batch *b, int T, int chunk, cudaStream_t s)
         return status(e);
     b->n_items = (int)b->h_items.size();
     b->cur_T = T;
-    b->cur_chunk = chunk;
+    b->cur_rows = rows;
     b->cur_engine = 1;
     return LBM_OK;
 }
 
-static int prepare(lbm_batch *b, int T, int chunk, cudaStream_t s)
+static int prepare(lbm_batch *b, int T, const Rows &rows, cudaStream_t s)
 {
     if (rw_engine(b, T))
-        return rbatch_items(b, T, chunk, s);
+        return rbatch_items(b, T, rows, s);
     if (b->cur_engine != 0) {
         b->cur_T = 0; // force a rebuild of the shared-memory wavefront's list
         b->cur_engine = 0;
     }
-    return batch_items(b, T, chunk, s);
+    return batch_items(b, T, rows, s);
 }
 
-static bool prepared(const lbm_batch *b, int T, int chunk)
+static bool prepared(const lbm_batch *b, int T, const Rows &rows)
 {
-    return b->cur_T == T && b->cur_chunk == chunk && b->cur_engine == (rw_engine(b, T) ? 1 : 0);
+    return b->cur_T == T && b->cur_rows == rows && b->cur_engine == (rw_engine(b, T) ? 1 : 0);
+}
+
+// Rows per item a configuration may use with depth T on the batch's engine.
+static bool rows_ok(const lbm_batch *b, int T, int ch)
+{
+    return ch >= 8 && ch >= 2 * T && ch <= 128 && (rw_engine(b, T) ? ch <= 32 : ch >= 16);
 }
 
 static int batch_launch_one(lbm_batch *b, int T, int parity, cudaStream_t s)
@@ -416,7 +471,8 @@ int lbm_batch_create(const lbm_params *common, const lbm_domain *domains, int n,
         hd.rw = tma && make_map_planes(&hd.rtmf[0], dm.f_a, es, dm.W, dm.H, dm.pitch, w.plane, 64 + 16 / es) &&
                 make_map_planes(&hd.rtmf[1], dm.f_b, es, dm.W, dm.H, dm.pitch, w.plane, 64 + 16 / es) &&
                 make_map_mask(&hd.rtmm, dm.mask, dm.W, dm.H, dm.mask_pitch, 80);
-        // bound on the work items of any (T, chunk >= 8) configuration of either engine
+        b->class_count[size_class(dm.W, dm.H)] += 1;
+        // bound on the work items of any (T, rows >= 8 or >= 4) configuration of either engine
         max_items += ((dm.W + (kBatchNX - 16) - 1) / (kBatchNX - 16)) * ((dm.H + 7) / 8) +
                      ((dm.W + 51) / 52) * ((dm.H + 3) / 4);
     }
@@ -426,7 +482,7 @@ int lbm_batch_create(const lbm_params *common, const lbm_domain *domains, int n,
         b->rw_all = b->rw_all && hd.rw;
     if (b->rw_all) {
         b->tuned_T = 2;
-        b->tuned_chunk = 16;
+        b->tuned_rows = uniform_rows(16);
     }
     cudaError_t e = cudaMalloc(&b->d_doms, sizeof(BatchDomain) * n);
     if (e == cudaSuccess)
@@ -464,11 +520,15 @@ int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in
     if (!b || n_steps < 0 || T < 0 || T > 8)
         return LBM_ERR_ARG;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    int chunk = b->tuned_chunk;
     if (T == 0)
         T = b->tuned_T;
     if (T != 1 && T != 2 && T != 4 && T != 8)
         return LBM_ERR_UNSUPPORTED;
+    // the tuned rows per class where they suit T and the engine, else the default
+    Rows chunk = b->tuned_rows;
+    for (int c = 0; c < LBM_BATCH_SIZE_CLASSES; ++c)
+        if (!rows_ok(b, T, chunk.r[c]))
+            chunk.r[c] = rw_engine(b, T) ? (T <= 2 ? 16 : 24) : 64;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaStreamIsCapturing(s, &cs);
     const bool capturing = cs != cudaStreamCaptureStatusNone;
@@ -482,7 +542,7 @@ int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in
     int done = 0, parity = 0;
     const int pairs = n_steps / (2 * T);
     if (pairs > 0 && !capturing) {
-        if (!b->exec || b->exec_T != T || b->exec_chunk != chunk) {
+        if (!b->exec || b->exec_T != T || b->exec_rows != chunk) {
             if (b->exec) {
                 cudaGraphExecDestroy(b->exec);
                 b->exec = nullptr;
@@ -505,7 +565,7 @@ int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in
             if (e != cudaSuccess)
                 return status(e);
             b->exec_T = T;
-            b->exec_chunk = chunk;
+            b->exec_rows = chunk;
         }
         for (int i = 0; i < pairs; ++i) {
             cudaError_t e = cudaGraphLaunch(b->exec, s);
@@ -518,10 +578,14 @@ int lbm_batch_run(lbm_batch *b, int n_steps, int T, void *stream, int *result_in
         // remaining steps: launches of depth T, then the largest supported depth that fits
         const int left = n_steps - done;
         const int t = left >= T ? T : (left >= 4 ? 4 : (left >= 2 ? 2 : 1));
-        if (!prepared(b, t, chunk)) {
+        Rows ct = chunk;
+        for (int c = 0; c < LBM_BATCH_SIZE_CLASSES; ++c)
+            if (!rows_ok(b, t, ct.r[c]))
+                ct.r[c] = rw_engine(b, t) ? (t <= 2 ? 16 : 24) : 64;
+        if (!prepared(b, t, ct)) {
             if (capturing)
                 return LBM_ERR_ARG;
-            int rc = prepare(b, t, chunk, s);
+            int rc = prepare(b, t, ct, s);
             if (rc)
                 return rc;
         }
@@ -564,6 +628,33 @@ int lbm_batch_run_separate(lbm_batch *b, int n_steps, int T, void *stream, int *
     return LBM_OK;
 }
 
+} // extern "C"
+
+namespace lbm {
+// Device time of one step of configuration (T, rows): two warm-up launches, then
+// `n` timed launches (ms per step), or a negative status.
+static float time_config(lbm_batch *b, int T, const Rows &rows, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1,
+                         int n, int *rc_out)
+{
+    int rc = prepare(b, T, rows, s);
+    for (int w = 0; !rc && w < 2; ++w)
+        rc = batch_launch_one(b, T, w & 1, s);
+    cudaEventRecord(e0, s);
+    for (int w = 0; !rc && w < n; ++w)
+        rc = batch_launch_one(b, T, w & 1, s);
+    cudaEventRecord(e1, s);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (!rc && e != cudaSuccess)
+        rc = status(e);
+    *rc_out = rc;
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms / ((float)n * T);
+}
+} // namespace lbm
+
+extern "C" {
+
 int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk)
 {
     if (!b)
@@ -572,46 +663,94 @@ int lbm_batch_autotune(lbm_batch *b, void *stream, int *best_T, int *best_chunk)
     const int Ts[] = {1, 2, 4, 8};
     const int chunks[] = {8, 16, 24, 32, 64, 128};
     float best = 1e30f;
-    int bT = 4, bC = 64;
+    int bT = b->tuned_T;
+    Rows bR = b->tuned_rows;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    int rc = LBM_OK;
     for (int T : Ts) {
+        // one height for every class first
+        float bt = 1e30f;
+        Rows br = uniform_rows(0);
         for (int ch : chunks) {
-            if (ch < 2 * T || (rw_engine(b, T) ? ch > 32 : ch < 16))
+            if (!rows_ok(b, T, ch))
                 continue;
-            int rc = prepare(b, T, ch, s);
+            const float t = time_config(b, T, uniform_rows(ch), s, e0, e1, 4, &rc);
             if (rc)
-                return rc;
-            for (int w = 0; w < 2; ++w)
-                if ((rc = batch_launch_one(b, T, w & 1, s)))
-                    return rc;
-            cudaEventRecord(e0, s);
-            for (int w = 0; w < 4; ++w)
-                if ((rc = batch_launch_one(b, T, w & 1, s)))
-                    return rc;
-            cudaEventRecord(e1, s);
-            cudaError_t e = cudaEventSynchronize(e1);
-            if (e != cudaSuccess)
-                return status(e);
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            const float per_step = ms / (4.0f * T);
-            if (per_step < best) {
-                best = per_step;
-                bT = T;
-                bC = ch;
+                break;
+            if (t < bt) {
+                bt = t;
+                br = uniform_rows(ch);
             }
+        }
+        if (rc)
+            break;
+        if (br.r[0] == 0)
+            continue;
+        // then each populated size class in turn, the others held at their best
+        for (int c = 0; c < LBM_BATCH_SIZE_CLASSES && !rc; ++c) {
+            if (b->class_count[c] == 0)
+                continue;
+            for (int ch : chunks) {
+                if (!rows_ok(b, T, ch) || ch == br.r[c])
+                    continue;
+                Rows cand = br;
+                cand.r[c] = ch;
+                const float t = time_config(b, T, cand, s, e0, e1, 4, &rc);
+                if (rc)
+                    break;
+                if (t < 0.98f * bt) { // a clear gain: the class is a part of the launch
+                    bt = t;
+                    br = cand;
+                }
+            }
+        }
+        if (!rc && bt < best) {
+            best = bt;
+            bT = T;
+            bR = br;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (rc)
+        return rc;
     b->tuned_T = bT;
-    b->tuned_chunk = bC;
+    b->tuned_rows = bR;
     if (best_T)
         *best_T = bT;
-    if (best_chunk)
-        *best_chunk = bC;
+    if (best_chunk) { // rows of the largest populated class
+        int c = LBM_BATCH_SIZE_CLASSES - 1;
+        while (c > 0 && b->class_count[c] == 0)
+            --c;
+        *best_chunk = bR.r[c];
+    }
+    return LBM_OK;
+}
+
+int lbm_batch_get_tiles(const lbm_batch *b, int *T, int *rows)
+{
+    if (!b || !T || !rows)
+        return LBM_ERR_ARG;
+    *T = b->tuned_T;
+    for (int c = 0; c < LBM_BATCH_SIZE_CLASSES; ++c)
+        rows[c] = b->tuned_rows.r[c];
+    return LBM_OK;
+}
+
+int lbm_batch_set_tiles(lbm_batch *b, int T, const int *rows)
+{
+    if (!b || !rows || (T != 1 && T != 2 && T != 4 && T != 8))
+        return LBM_ERR_ARG;
+    Rows r;
+    for (int c = 0; c < LBM_BATCH_SIZE_CLASSES; ++c) {
+        if (!rows_ok(b, T, rows[c]))
+            return LBM_ERR_ARG;
+        r.r[c] = rows[c];
+    }
+    b->tuned_T = T;
+    b->tuned_rows = r;
     return LBM_OK;
 }
 

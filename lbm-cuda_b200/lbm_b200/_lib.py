@@ -54,6 +54,8 @@ SIGNATURES = {
     "lbm_batch_run": ([_P, _I, _I, _P, _IP], _I),
     "lbm_batch_run_separate": ([_P, _I, _I, _P, _IP], _I),
     "lbm_batch_autotune": ([_P, _P, _IP, _IP], _I),
+    "lbm_batch_get_tiles": ([_P, _IP, _IP], _I),
+    "lbm_batch_set_tiles": ([_P, _I, _IP], _I),
     "lbm_error_string": ([_I], C.c_char_p),
     "lbm_version": ([], _I),
 }

@@ -7,6 +7,8 @@ import ctypes as C
 from ._lib import call
 from .solver import Params, default_params
 
+SIZE_CLASSES = 3  # LBM_BATCH_SIZE_CLASSES: < 2^17 cells, < 2^19, larger
+
 
 class Domain(C.Structure):
     """Mirror of ``lbm_domain`` (include/lbm_b200.h)."""
@@ -66,9 +68,23 @@ class Batch:
         return out.value
 
     def autotune(self, stream=None):
-        """Pick (T, rows per work item); returns them.  Synchronous; advances the states."""
+        """Pick T and the rows per work item of every size class; returns (T, rows of
+        the largest populated class) (``tiles()`` gives all).  Synchronous;
+        advances the states."""
         from . import _stream
 
         t, c = C.c_int(0), C.c_int(0)
         call("lbm_batch_autotune", self._h, _stream(stream), C.byref(t), C.byref(c))
         return t.value, c.value
+
+    def tiles(self):
+        """(T, [rows per item of each size class]) that run(T=0) uses."""
+        t = C.c_int(0)
+        rows = (C.c_int * SIZE_CLASSES)()
+        call("lbm_batch_get_tiles", self._h, C.byref(t), rows)
+        return t.value, list(rows)
+
+    def set_tiles(self, T: int, rows) -> None:
+        """Sets the configuration run(T=0) uses: depth T and rows per class."""
+        arr = (C.c_int * SIZE_CLASSES)(*[int(r) for r in rows])
+        call("lbm_batch_set_tiles", self._h, int(T), arr)

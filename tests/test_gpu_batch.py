@@ -86,3 +86,62 @@ def test_autotune_then_run():
     assert which in (0, 1)
     for d in doms:
         assert torch.isfinite((d["f_b"] if which else d["f_a"])).all()
+
+
+CLASS_SIZES = [(70, 48), (256, 96), (512, 320), (1024, 640)]  # size classes 0, 0, 1, 2
+
+
+def _class_domains(aligned, seed):
+    doms = []
+    for i, (W, H) in enumerate(CLASS_SIZES):
+        m = I.random_discs_mask(W, H, 2, 3.0, 8.0, seed + i)
+        pitch = ((W + 15) // 16) * 16 if aligned else W
+        fa = torch.zeros((9, H, pitch), device="cuda")
+        fa[:, :, :W] = dev(I.perturbed_state(W, H, seed + 50 + i, amp=0.02))
+        mk = torch.zeros((H, pitch), dtype=torch.uint8, device="cuda")
+        mk[:, :W] = dev(m)
+        doms.append(dict(W=W, H=H, pitch=pitch if aligned else 0, mask_pitch=pitch if aligned else 0, f_a=fa,
+                         f_b=fa.clone(), mask=mk, u_in=0.03 + 0.01 * i))
+    return doms
+
+
+@pytest.mark.parametrize("aligned,T,cfgs", [
+    (True, 2, ([16, 16, 16], [8, 24, 32], [32, 8, 16])),       # register wavefront items
+    (False, 4, ([64, 64, 64], [16, 32, 128], [128, 16, 64])),  # shared-memory wavefront items
+])
+def test_per_class_tile_rows_give_the_same_states(aligned, T, cfgs):
+    """The rows per work item of each size class only change how the domains are
+    cut into items: the register-wavefront engine gives the same states bit for
+    bit; the shared-memory engine's cells near an item boundary can round
+    differently (a few ulps)."""
+    outs = []
+    for rows in cfgs:
+        doms = _class_domains(aligned, 300)
+        B = Batch(doms, storage=SV.STORE_F32, **PHYS)
+        B.set_tiles(T, rows)
+        assert B.tiles() == (T, list(rows))
+        which = B.run(6 * T, 0)
+        outs.append([host((d["f_b"] if which else d["f_a"])[:, :, :d["W"]].contiguous()) for d in doms])
+        B.close()
+    for other in outs[1:]:
+        for a, b in zip(outs[0], other):
+            if aligned:
+                assert np.array_equal(a, b)
+            else:
+                assert rel_l2(a, b) < 1e-6
+
+
+def test_autotune_per_class_rows_and_validation():
+    doms = _class_domains(True, 400)
+    B = Batch(doms, storage=SV.STORE_F32, **PHYS)
+    T, chunk = B.autotune()
+    T2, rows = B.tiles()
+    assert T2 == T and len(rows) == 3 and rows[2] == chunk
+    assert all(8 <= r and r >= 2 * T for r in rows)
+    with pytest.raises(Exception):
+        B.set_tiles(2, [4, 16, 16])  # below the smallest item height
+    with pytest.raises(Exception):
+        B.set_tiles(3, [16, 16, 16])  # depth not built for batches
+    which = B.run(2 * T, 0)
+    for d in doms:
+        assert torch.isfinite(d["f_b"] if which else d["f_a"]).all()
