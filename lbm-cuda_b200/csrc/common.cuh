@@ -185,6 +185,18 @@ __device__ __forceinline__ void prefetch_tmap(const CUtensorMap *map)
     asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
+// Programmatic dependent launch: let the next kernel of the stream be scheduled
+// (pdl_trigger), and wait until the previous one has completed with its memory
+// visible (pdl_wait; a no-op for a kernel launched without the attribute).
+__device__ __forceinline__ void pdl_trigger()
+{
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+__device__ __forceinline__ void pdl_wait()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 __host__ __device__ constexpr int round_up(int a, int b)
 {
     return (a + b - 1) / b * b;

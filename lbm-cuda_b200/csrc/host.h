@@ -6,6 +6,7 @@
 #include <cudaTypedefs.h>
 #include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
+#include <stdlib.h>
 
 #include <atomic>
 
@@ -81,6 +82,31 @@ inline bool make_map_mask(CUtensorMap *m, const void *base, int W, int H, int pi
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
+}
+
+// Launch with programmatic dependent launch: the kernel may be scheduled while
+// the previous kernel in the stream drains; it must execute griddepcontrol.wait
+// (pdl_wait) before touching anything that kernel writes.  LBM_PDL=0 in the
+// environment launches plainly.
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args &&...args)
+{
+    static const bool on = [] {
+        const char *e = getenv("LBM_PDL");
+        return !(e && e[0] == '0');
+    }();
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = on ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args &&>(args)...);
 }
 
 inline int status(cudaError_t e)

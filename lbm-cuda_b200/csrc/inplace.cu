@@ -27,7 +27,11 @@
 //
 // One thread per cell, 128 x 2 cells per CTA; the 3 x 3 mask neighbourhood is
 // read per cell (L1-resident).  Memory traffic: 72 B per update in FP32, like
-// the ping-pong streaming kernel, with half the state memory.
+// the ping-pong streaming kernel, with half the state memory.  The two kernels
+// of a pair of steps run back to back: each is launched with programmatic
+// dependent launch (its CTAs are scheduled while the previous step drains and
+// wait in griddepcontrol.wait until that step's stores are visible), which
+// hides the gap between consecutive one-step launches.
 #include <type_traits>
 
 #include "dispatch.cuh"
@@ -170,6 +174,8 @@ __device__ __forceinline__ void inplace_cell(const InplaceParams &p, int x, int 
 template <class Ph, class St, bool LID, bool LOCAL>
 __global__ void __launch_bounds__(256) inplace_kernel(const __grid_constant__ InplaceParams p)
 {
+    pdl_trigger();
+    pdl_wait(); // the previous step's kernel has completed: its stores are visible
     const int x = blockIdx.x * 128 + threadIdx.x;
     const int y = blockIdx.y * 2 + threadIdx.y;
     if (x < p.W && y < p.H)
@@ -195,6 +201,8 @@ __global__ void __launch_bounds__(256, LBM_INPLACE_MINB) inplace_vec_kernel(cons
 {
     using E = typename St::T;
     using V = typename Raw4<E>::type;
+    pdl_trigger();
+    pdl_wait(); // the previous step's kernel has completed: its stores are visible
     const int W = p.W, H = p.H;
     const int x4 = (blockIdx.x * 64 + threadIdx.x) * 4;
     const int y = blockIdx.y * 4 + threadIdx.y;
@@ -314,18 +322,12 @@ template <class Ph, class St, bool LID> static int inplace_pair(const InplacePar
     const bool vec = p.W % 4 == 0 && al16(p.f) && al16(p.mask) && (!p.ux || (al16(p.ux) && al16(p.uy) && al16(p.rho)));
     if (vec) {
         const dim3 block(64, 4), grid((p.W / 4 + 63) / 64, (p.H + 3) / 4);
-        if (local)
-            inplace_vec_kernel<Ph, St, LID, true><<<grid, block, 0, s>>>(p);
-        else
-            inplace_vec_kernel<Ph, St, LID, false><<<grid, block, 0, s>>>(p);
-        return status(cudaGetLastError());
+        return status(local ? launch_pdl(inplace_vec_kernel<Ph, St, LID, true>, grid, block, 0, s, p)
+                            : launch_pdl(inplace_vec_kernel<Ph, St, LID, false>, grid, block, 0, s, p));
     }
     const dim3 block(128, 2), grid((p.W + 127) / 128, (p.H + 1) / 2);
-    if (local)
-        inplace_kernel<Ph, St, LID, true><<<grid, block, 0, s>>>(p);
-    else
-        inplace_kernel<Ph, St, LID, false><<<grid, block, 0, s>>>(p);
-    return status(cudaGetLastError());
+    return status(local ? launch_pdl(inplace_kernel<Ph, St, LID, true>, grid, block, 0, s, p)
+                        : launch_pdl(inplace_kernel<Ph, St, LID, false>, grid, block, 0, s, p));
 }
 
 template <class St> static int inplace_variant(int variant, const InplaceParams &p, bool local, cudaStream_t s)

@@ -744,6 +744,10 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
     rwave_kernel(const __grid_constant__ WaveParams p, const __grid_constant__ CUtensorMap tmf,
                  const __grid_constant__ CUtensorMap tmm)
 {
+    // launched with programmatic dependent launch: wait for the previous launch's
+    // stores (its output is this launch's input) before the first row load
+    pdl_trigger();
+    pdl_wait();
     // output rectangle [rx0, rx1) x [ry0, ry1) (the whole domain unless set)
     const int rx0 = p.rx1 > 0 ? p.rx0 : 0, rx1 = p.rx1 > 0 ? p.rx1 : p.W;
     const int ry0 = p.ry1 > 0 ? p.ry0 : 0, ry1 = p.ry1 > 0 ? p.ry1 : p.H;
@@ -837,8 +841,7 @@ template <class C> int launch_rwave(WaveParams p, cudaStream_t s)
     p.use_tma = 1;
     const RwItems it = rw_items(Wr, Hr, C::CW, C::PADL, p.chunk);
     const int grid = (it.n_items + C::NW - 1) / C::NW;
-    rwave_kernel<C><<<grid, 32 * C::NW, C::SMEM, s>>>(p, tmf, tmm);
-    return status(cudaGetLastError());
+    return status(launch_pdl(rwave_kernel<C>, dim3(grid), dim3(32 * C::NW), (size_t)C::SMEM, s, p, tmf, tmm));
 }
 
 } // namespace lbm
