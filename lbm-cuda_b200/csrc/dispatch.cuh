@@ -26,8 +26,7 @@ template <class C> int launch_stream(WaveParams p, cudaStream_t s)
         p.err = device_error_word();
     dim3 grid((p.W + 127) / 128, (p.H + 3) / 4);
     dim3 block(32, 4);
-    stream_kernel<C><<<grid, block, 0, s>>>(p);
-    return status(cudaGetLastError());
+    return status(launch_pdl(stream_kernel<C>, grid, block, 0, s, p));
 }
 
 inline bool stream_ok(const WaveParams &p)

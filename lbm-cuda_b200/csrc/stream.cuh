@@ -148,6 +148,8 @@ template <class C> __global__ void __launch_bounds__(128, 4) stream_kernel(const
     using E = typename C::E;
     using V = typename Raw4<E>::type;
     using Ph = typename C::Ph;
+    pdl_trigger();
+    pdl_wait(); // launched with programmatic dependent launch: the previous step's stores first
     const int W = p.W, H = p.H;
     const int lane = threadIdx.x;
     const int x4 = 4 * (blockIdx.x * 32 + lane);

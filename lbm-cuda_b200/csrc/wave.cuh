@@ -503,6 +503,8 @@ __global__ void __launch_bounds__(C::NX, C::MINB)
     wave_kernel(const __grid_constant__ WaveParams p, const __grid_constant__ CUtensorMap tmf,
                 const __grid_constant__ CUtensorMap tmm)
 {
+    pdl_trigger();
+    pdl_wait(); // launched with programmatic dependent launch: the previous step's stores first
     wave_tile<C>(p, &tmf, &tmm, blockIdx.x, blockIdx.y, false);
 }
 

@@ -71,8 +71,7 @@ template <class C> int launch_wave(WaveParams p, cudaStream_t s)
               make_map_mask(&tmm, p.mask, p.W, p.H, p.mask_pitch, C::RWM);
     p.use_tma = tma ? 1 : 0;
     dim3 grid((p.W + C::CW - 1) / C::CW, (p.H + p.chunk - 1) / p.chunk);
-    wave_kernel<C><<<grid, C::NX, C::SMEM, s>>>(p, tmf, tmm);
-    return status(cudaGetLastError());
+    return status(launch_pdl(wave_kernel<C>, grid, dim3(C::NX), (size_t)C::SMEM, s, p, tmf, tmm));
 }
 
 } // namespace lbm
