@@ -102,6 +102,8 @@ __global__ void __launch_bounds__(C::NT, C::MINB) aa_tile_kernel(const __grid_co
                                                            const __grid_constant__ CUtensorMap tmm)
 {
     constexpr int T = C::T, SX = C::SX, SY = C::SY, CX = C::CX, CY = C::CY, SW = C::SW, PL = C::PL, MW = C::MW;
+    pdl_trigger();
+    pdl_wait(); // launched with programmatic dependent launch: the previous launch's stores first
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     float *S = reinterpret_cast<float *>(smem + C::OFF_F);

@@ -34,8 +34,7 @@ template <class C> int launch_aa(AaParams p, cudaStream_t s)
               make_map_mask(&tmm, p.mask, p.W, p.H, p.W, C::MW, C::SY);
     p.use_tma = tma ? 1 : 0;
     dim3 grid((p.W + C::CX - 1) / C::CX, (p.H + C::CY - 1) / C::CY);
-    aa_tile_kernel<C><<<grid, C::NT, C::SMEM, s>>>(p, tmf, tmm);
-    return status(cudaGetLastError());
+    return status(launch_pdl(aa_tile_kernel<C>, grid, dim3(C::NT), (size_t)C::SMEM, s, p, tmf, tmm));
 }
 
 // The tile kernel on an explicit 1-D grid (edge-only launches).
@@ -60,8 +59,7 @@ template <class C> int launch_aa_grid(AaParams p, int nblocks, cudaStream_t s)
         tma = make_map_planes(&tmf, p.f_in, 4, p.W, p.H, p.W, (long long)p.W * p.H, C::SW, C::SY) &&
               make_map_mask(&tmm, p.mask, p.W, p.H, p.W, C::MW, C::SY);
     p.use_tma = tma ? 1 : 0;
-    aa_tile_kernel<C><<<nblocks, C::NT, C::SMEM, s>>>(p, tmf, tmm);
-    return status(cudaGetLastError());
+    return status(launch_pdl(aa_tile_kernel<C>, dim3(nblocks), dim3(C::NT), (size_t)C::SMEM, s, p, tmf, tmm));
 }
 
 template <class Cfg, int MODE> static int aa_split(AaParams p, int T, cudaStream_t s, bool &done);
