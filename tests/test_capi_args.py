@@ -92,6 +92,20 @@ def test_solver_calls_refuse_bad_arguments(lib):
     assert lib.lbm_mlp_forward_act(P, 2, P, P, 10, None) == ERR_ARG
     assert lib.lbm_mlp_grad_act(P, -1, P, P, nul, 10, P, P, P, C.c_size_t(1 << 20), None) == ERR_ARG
     assert lib.lbm_mlp_pack_act(P, 7, P, 1.0, P, None) == ERR_ARG
+    # column-restricted launches: no handle, aliasing buffers, odd / empty / out-of-range columns
+    assert lib.lbm_run_columns(nul, P, P2, P, 2, 0, 64, None) == ERR_ARG
+    assert lib.lbm_run_columns(nul, P, P, P, 2, 0, 64, None) == ERR_ARG
+    # halo pack / unpack: no side, columns beyond the width, unknown storage, no buffer
+    assert lib.lbm_halo_pack(P, 64, 32, 0, -1, -1, 4, P2, None) == ERR_ARG
+    assert lib.lbm_halo_pack(P, 64, 32, 0, 62, -1, 4, P2, None) == ERR_ARG
+    assert lib.lbm_halo_pack(P, 64, 32, 9, 0, 60, 4, P2, None) == ERR_ARG
+    assert lib.lbm_halo_unpack(P, 64, 32, 0, 0, 60, 4, nul, None) == ERR_ARG
+    assert lib.lbm_halo_unpack(P, 64, 32, 0, 0, 60, 0, P2, None) == ERR_ARG
+    # batch tile configuration without a batch
+    rows = (C.c_int * 3)(16, 16, 16)
+    t = C.c_int(0)
+    assert lib.lbm_batch_get_tiles(nul, C.byref(t), rows) == ERR_ARG
+    assert lib.lbm_batch_set_tiles(nul, 2, rows) == ERR_ARG
     # the wait self-test: limit outside 1 .. 2^31, arrive not 0 / 1
     assert lib.lbm_selftest_wait_timeout(0, 0, None, None) == ERR_ARG
     assert lib.lbm_selftest_wait_timeout((1 << 31) + 1, 0, None, None) == ERR_ARG
