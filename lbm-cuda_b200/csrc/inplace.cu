@@ -209,15 +209,41 @@ __global__ void __launch_bounds__(256, LBM_INPLACE_MINB) inplace_vec_kernel(cons
     const int lane = threadIdx.x & 31;
     const bool xok = x4 < W && y < H;
     bool interior = xok && x4 >= 1 && x4 + 3 <= W - 3 && y >= 1 && y <= H - 2;
+    // The mask loads of the interior test and the population loads of the vector
+    // path are issued together, so that one memory latency covers both; a warp
+    // that turns out not to be interior drops the populations (its per-cell code
+    // loads them again, from cache).  The loads are predicated on the cell and
+    // its source row being inside the domain.
+    uint32_t any = 0;
     if (interior) {
-        uint32_t any = 0;
 #pragma unroll
         for (int dy = -1; dy <= 1; ++dy) {
             const uint8_t *m = p.mask + (long long)(y + dy) * W + x4;
             any |= *reinterpret_cast<const uint32_t *>(m) | m[-1] | m[4];
         }
-        interior = any == 0;
     }
+    const long long N = (long long)W * H;
+    const long long id = (long long)y * W + x4;
+    E *f = reinterpret_cast<E *>(p.f);
+    V raw[9];
+    float edge[9];
+#pragma unroll
+    for (int q = 0; q < 9; ++q) {
+        edge[q] = 0.0f;
+        if (LOCAL) {
+            raw[q] = ld4<E>(f + (q == 0 ? 0 : opp(q)) * N + id, xok);
+        } else {
+            const int sy = y - cy(q);
+            const bool rok = xok && sy >= 0 && sy < H;
+            const E *src = f + q * N + id - (long long)cy(q) * W;
+            raw[q] = ld4<E>(src, rok);
+            if (cx(q) > 0) // column x4 - 1, for lane 0
+                edge[q] = ld1<St>(src - 1, rok && lane == 0 && x4 >= 1, q);
+            else if (cx(q) < 0) // column x4 + 4, for lane 31
+                edge[q] = ld1<St>(src + 4, rok && lane == 31 && x4 + 4 < W, q);
+        }
+    }
+    interior = interior && any == 0;
     if (!__all_sync(0xffffffffu, interior)) {
         if (xok) {
 #pragma unroll 1
@@ -226,22 +252,17 @@ __global__ void __launch_bounds__(256, LBM_INPLACE_MINB) inplace_vec_kernel(cons
         }
         return;
     }
-    const long long N = (long long)W * H;
-    const long long id = (long long)y * W + x4;
-    E *f = reinterpret_cast<E *>(p.f);
     float g[4][9];
 #pragma unroll
     for (int q = 0; q < 9; ++q) {
         float o[4];
         if (LOCAL) {
-            const int pq = q == 0 ? 0 : opp(q);
-            unpack4<St>(ld4<E>(f + pq * N + id, true), pq, o);
+            unpack4<St>(raw[q], q == 0 ? 0 : opp(q), o);
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 g[j][q] = o[j];
         } else {
-            const E *src = f + q * N + id - (long long)cy(q) * W;
-            unpack4<St>(ld4<E>(src, true), q, o);
+            unpack4<St>(raw[q], q, o);
             if (cx(q) == 0) {
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
@@ -249,7 +270,7 @@ __global__ void __launch_bounds__(256, LBM_INPLACE_MINB) inplace_vec_kernel(cons
             } else if (cx(q) > 0) { // column x - 1
                 float prev = __shfl_up_sync(0xffffffffu, o[3], 1);
                 if (lane == 0)
-                    prev = ld1<St>(src - 1, true, q);
+                    prev = edge[q];
                 g[0][q] = prev;
                 g[1][q] = o[0];
                 g[2][q] = o[1];
@@ -257,7 +278,7 @@ __global__ void __launch_bounds__(256, LBM_INPLACE_MINB) inplace_vec_kernel(cons
             } else { // column x + 1
                 float next = __shfl_down_sync(0xffffffffu, o[0], 1);
                 if (lane == 31)
-                    next = ld1<St>(src + 4, true, q);
+                    next = edge[q];
                 g[0][q] = o[1];
                 g[1][q] = o[2];
                 g[2][q] = o[3];
