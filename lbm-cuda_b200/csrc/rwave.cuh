@@ -246,7 +246,10 @@ __host__ __device__ __forceinline__ void codes_from_bytes(const uint32_t (&raw)[
 // left and right ends take the generic body on every row (inlet, outlet, out-
 // of-domain columns), so they come first in launch order and in chunks of half
 // the height; the hardware starts CTAs in index order as earlier ones finish,
-// which lets the cheaper items fill in behind them.
+// which lets the cheaper items fill in behind them.  The other items follow
+// window by window (vertically adjacent chunks of a window run at about the
+// same time): on the 4096 x 1024 cylinder at T = 2, 118.3 GLUPS against 115.3
+// with the chunks of a row band consecutive, at the same DRAM traffic.
 struct RwItems {
     int nwin, wr, nedge, che, nche, nch, n_edge_items, n_items;
 };
@@ -278,9 +281,11 @@ __host__ __device__ __forceinline__ void rw_item(const RwItems &it, int item, in
         ya = k * it.che;
         yb = min(H, ya + it.che);
     } else {
-        const int j = item - it.n_edge_items, nmid = it.nwin - it.nedge;
-        win = 1 + j % nmid;
-        ya = (j / nmid) * chunk;
+        // window by window: consecutive items are vertically adjacent row chunks
+        // of one window
+        const int j = item - it.n_edge_items;
+        win = 1 + j / it.nch;
+        ya = (j % it.nch) * chunk;
         yb = min(H, ya + chunk);
     }
 }
