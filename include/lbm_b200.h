@@ -139,7 +139,11 @@ void lbm_params_default(lbm_params *p, int W, int H);
 
 /* Validate the parameters and allocate the handle and its small reduction
  * scratch (the only entry point that allocates device memory); lbm_destroy
- * frees them and lbm_run's cached graph. */
+ * frees them and lbm_run's cached graph.  When the planes' rows are a multiple
+ * of 16 bytes but W is not a multiple of 16 (and x is not periodic, storage not
+ * FP64), the handle also holds a copy of the mask with rows padded to a multiple
+ * of 16 bytes (H * roundup(W, 16) bytes): the register wavefront kernel's TMA row
+ * loads need that stride. */
 int lbm_create(const lbm_params *p, lbm_handle **out);
 int lbm_destroy(lbm_handle *h);
 
@@ -153,7 +157,9 @@ int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *
  * (1 <= T <= 8; FP64 storage: one step per launch whatever T).  The stored
  * state is post-collision populations (the lbm_core4.cu convention).  u, v, rho
  * of the last step are written when the pointers are non-NULL.  *result_in_b =
- * 1 when the final state is in f_b.
+ * 1 when the final state is in f_b.  A handle with a padded mask copy (see
+ * lbm_create) copies the mask into it first, on `stream`: two lbm_run calls on
+ * such a handle must not overlap on the GPU.
  * Graph cache: when at least three whole pairs of T-step launches precede the
  * last launch, the handle captures one pair as a CUDA graph and replays it, so
  * a small domain pays one graph launch per pair; the results are bit-identical

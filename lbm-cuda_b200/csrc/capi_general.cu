@@ -27,6 +27,11 @@ struct lbm_handle {
     lbm::PairGraph graphs[2];
     unsigned long long uses;
     std::atomic<int> g_busy; // held by the lbm_run call using the graphs (others launch plainly)
+    // Domains whose planes suit the register wavefront's TMA row loads but whose width
+    // is not a multiple of 16 (the mask rows' stride cannot be a TMA stride): lbm_run
+    // copies the mask into this buffer of 16-byte aligned rows first
+    uint8_t *mask_pad;
+    int mask_pad_pitch;
 };
 
 namespace lbm {
@@ -356,6 +361,16 @@ int lbm_create(const lbm_params *p, lbm_handle **out)
         free(h);
         return status(e);
     }
+    const int es = elem_bytes(p->storage);
+    if (p->storage != LBM_STORE_F64 && p->bc_left != LBM_BC_PERIODIC && (p->W * es) % 16 == 0 && p->W % 16 != 0) {
+        h->mask_pad_pitch = (p->W + 15) / 16 * 16;
+        e = cudaMalloc(&h->mask_pad, (size_t)h->mask_pad_pitch * p->H);
+        if (e != cudaSuccess) {
+            cudaFree(h->partials);
+            free(h);
+            return status(e);
+        }
+    }
     *out = h;
     return LBM_OK;
 }
@@ -370,6 +385,11 @@ int lbm_destroy(lbm_handle *h)
     if (h->cap)
         cudaStreamDestroy(h->cap);
     cudaError_t e = cudaFree(h->partials);
+    if (h->mask_pad) {
+        const cudaError_t e2 = cudaFree(h->mask_pad);
+        if (e == cudaSuccess)
+            e = e2;
+    }
     free(h);
     return status(e);
 }
@@ -418,7 +438,7 @@ static int run_launch(lbm_handle *h, void *src, void *dst, const uint8_t *mask, 
     wp.H = h->p.H;
     wp.pitch = h->p.W;
     wp.plane = (long long)h->p.W * h->p.H;
-    wp.mask_pitch = h->p.W;
+    wp.mask_pitch = (h->mask_pad && mask == h->mask_pad) ? h->mask_pad_pitch : h->p.W;
     wp.chunk = 0;
     wp.bc_left = h->p.bc_left;
     wp.bc_right = h->p.bc_right;
@@ -518,6 +538,14 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
         T = 1; // the FP64 kernel advances one step per launch
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     int launches = 0, done = 0, rc = LBM_OK;
+    if (h->mask_pad && n_steps > 0) {
+        // rows of 16-byte aligned pitch for the TMA row loads (one copy per call)
+        cudaError_t e = cudaMemcpy2DAsync(h->mask_pad, h->mask_pad_pitch, mask, h->p.W, h->p.W, h->p.H,
+                                          cudaMemcpyDeviceToDevice, s);
+        if (e != cudaSuccess)
+            return status(e);
+        mask = h->mask_pad;
+    }
     // Whole pairs of T-step launches before the last launch replay from a CUDA
     // graph captured once per (f_a, f_b, mask, T): the host loop of small domains
     // costs a launch per pair instead of two kernel launches.  The first pair runs
