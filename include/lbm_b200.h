@@ -154,7 +154,9 @@ size_t lbm_state_bytes(const lbm_handle *h);
 int lbm_init_equilibrium(lbm_handle *h, void *f, const float *rho, const float *ux, const float *uy, void *stream);
 
 /* n_steps pull steps in ping-pong order starting from f_a, fused T per launch
- * (1 <= T <= 8; FP64 storage: one step per launch whatever T).  The stored
+ * (1 <= T <= 8; FP64 storage, and x-periodic domains without the learned
+ * closure whose buffers suit the streaming kernel, one step per launch whatever
+ * T: it is the faster kernel there).  The stored
  * state is post-collision populations (the lbm_core4.cu convention).  u, v, rho
  * of the last step are written when the pointers are non-NULL.  *result_in_b =
  * 1 when the final state is in f_b.  A handle with a padded mask copy (see
@@ -178,7 +180,7 @@ int lbm_run(lbm_handle *h, void *f_a, void *f_b, const uint8_t *mask, int n_step
  * contents (no counterpart in the reference, whose kernels cover the whole
  * domain).  The x-slab decomposition computes a rank's edge columns with it
  * first, sends them while the interior columns compute, then fills its halos.
- * Needs the register wavefront kernel: T in {2, 4, 6} (1 .. 4 with the learned
+ * Needs the register wavefront kernel: 2 <= T <= 6 (1 .. 4 with the learned
  * closure), TMA-aligned buffers (16-byte bases, W a multiple of 4 elements and
  * of 16 mask bytes) and x not periodic; otherwise LBM_ERR_UNSUPPORTED. */
 int lbm_run_columns(lbm_handle *h, const void *src, void *dst, const uint8_t *mask, int T, int x0, int x1,

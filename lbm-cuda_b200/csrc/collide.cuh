@@ -317,7 +317,10 @@ __device__ __forceinline__ void collide_bf(float (&f)[9], bool inlet, float lu, 
         s = (kZh && inlet && !Ph::kInletSmag) ? k.s_nu : sm;
     }
     if (Ph::kMrt) {
-        const bool cons = Ph::kClampU || kZh; // conserved moments may be replaced
+        // conserved moments replaced by the clamps or the Zou-He inlet; without
+        // them d0 = d3 = d5 = 0 exactly, as in collide_multi, so that a cell
+        // gets the same bits from either function
+        const bool cons = Ph::kClampU || (kZh && inlet);
         const float d0 = cons ? rho - r : 0.0f;
         const float d3 = cons ? jx - m3 : 0.0f;
         const float d5 = cons ? jy - m5 : 0.0f;

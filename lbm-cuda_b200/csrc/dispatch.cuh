@@ -81,12 +81,19 @@ int launch_step(const WaveParams &p, int T, cudaStream_t s)
 {
     if (T == 1 && stream_ok(p))
         return launch_stream<StreamCfg<Ph, St, MODE, LID>>(p, s);
-    if (rwave_ok<typename St::T>(p, T, MODE)) {
-        if (T == 2)
+    if (T >= 2 && rwave_ok<typename St::T>(p, T, MODE)) {
+        switch (T) {
+        case 2:
             return launch_rwave<RwCfg<2, 1, LBM_RW2_P, Ph, St, MODE, LID, true, LBM_RW2_MINB, LBM_RW2_LAG>>(p, s);
-        if (T == 4)
+        case 3:
+            return launch_rwave<RwCfg<3, 1, 2, Ph, St, MODE, LID, true>>(p, s);
+        case 4:
             return launch_rwave<RwCfg<4, 1, 2, Ph, St, MODE, LID, false>>(p, s);
-        return launch_rwave<RwCfg<6, 1, 2, Ph, St, MODE, LID, false>>(p, s);
+        case 5:
+            return launch_rwave<RwCfg<5, 1, 2, Ph, St, MODE, LID, false>>(p, s);
+        default:
+            return launch_rwave<RwCfg<6, 1, 2, Ph, St, MODE, LID, false>>(p, s);
+        }
     }
     switch (T) {
     case 1:

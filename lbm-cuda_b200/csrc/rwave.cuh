@@ -767,11 +767,11 @@ __global__ void __launch_bounds__(32 * C::NW, C::MINB)
 
 // Launch constraints: TMA-aligned planes and mask (16-byte base, pitches and
 // plane strides multiples of 16 bytes), no periodic x (the TMA boxes do not
-// wrap), T in {2, 4, 6}.
+// wrap), 2 <= T <= 6 (1 <= T <= 6 for the learned closure).
 template <class E> inline bool rwave_ok(const WaveParams &p, int T, int mode, bool any_T = false)
 {
     const int es = (int)sizeof(E);
-    if (any_T ? !(T >= 1 && T <= 6) : !(T == 2 || T == 4 || T == 6))
+    if (any_T ? !(T >= 1 && T <= 6) : !(T >= 2 && T <= 6))
         return false;
     if (!any_T)
         if (const char *e = getenv("LBM_KERNEL"))

@@ -62,7 +62,7 @@ def case_inputs(kind, W, H, seed=1):
     return m, f0
 
 
-@pytest.mark.parametrize("T", [1, 2, 4, 6, 8])
+@pytest.mark.parametrize("T", [1, 2, 3, 4, 5, 6, 8])
 @pytest.mark.parametrize("W,H", [(130, 66), (136, 66), (256, 96)])  # 136: rows padded for the TMA mask map
 @pytest.mark.parametrize("name", list(CASES))
 def test_general_vs_oracle(name, W, H, T):
