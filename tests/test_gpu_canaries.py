@@ -88,7 +88,7 @@ def test_dropins_stay_in_bounds(W, H):
 
 
 @pytest.mark.parametrize("storage,dtype", [(SV.STORE_F32, torch.float32), (SV.STORE_F16DEV, torch.float16)])
-@pytest.mark.parametrize("W,H", [(130, 66), (256, 96), (640, 200)])
+@pytest.mark.parametrize("W,H", [(130, 66), (256, 96), (640, 200), (600, 200)])  # 600: padded mask rows
 def test_general_solver_stays_in_bounds(W, H, storage, dtype):
     m, f0 = _case(W, H, 5)
     mask, fa, fb, mac = _arrays(W, H, m, f0, dtype)
@@ -96,7 +96,7 @@ def test_general_solver_stays_in_bounds(W, H, storage, dtype):
     SV.convert_state(f32, SV.STORE_F32, fa.t, storage)
     S = SV.Solver(W, H, storage=storage, cs_smag=0.1, u_in=0.05, s_nu=1.9)
     u = [g.t for g in mac]
-    for T in (1, 2, 4, 6, 8):
+    for T in (1, 2, 3, 4, 5, 6, 8):
         src = fa.t.clone()
         S.run(fa.t, fb.t, mask.t, T, T, *u)  # one launch: f_a is the source only
         torch.cuda.synchronize()
