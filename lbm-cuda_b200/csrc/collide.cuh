@@ -665,4 +665,118 @@ __device__ __forceinline__ void collide_pair(float2 (&f)[9], const Phys &k, floa
     }
 }
 
+// Two cells on the packed FP32x2 pipe in the reference's evaluation order:
+// collide_ref_bf without the Zou-He inlet (the inlet window keeps the scalar
+// form).  The sequential sums of moments_seq and the sums and products of
+// smag_rate, mrt_relax and bgk_relax are FADD2 / FMUL2 / FFMA2 in the same
+// order; the divisions and square roots stay per cell.  Rounding can differ
+// from the scalar form where the compiler contracts a product and a sum into
+// one FMA differently.  The clamps are applied only when a value is outside
+// its range, as in collide_pair.
+template <class Ph>
+__device__ __forceinline__ void collide_ref_pair(float2 (&f)[9], const Phys &k, float2 &r, float2 &u, float2 &v)
+{
+    static_assert(!Ph::kRuntime && Ph::kRefOrder, "reference-order compile-time physics only");
+    // moments_seq
+    float2 rr = f[0];
+#pragma unroll
+    for (int q = 1; q < 9; ++q)
+        rr = add2(rr, f[q]);
+    const float2 jx = add2(sub2(sub2(add2(sub2(f[1], f[3]), f[5]), f[6]), f[7]), f[8]);
+    const float2 jy = sub2(sub2(add2(add2(sub2(f[2], f[4]), f[5]), f[6]), f[7]), f[8]);
+    u = make_float2(jx.x / rr.x, jx.y / rr.y);
+    v = make_float2(jy.x / rr.x, jy.y / rr.y);
+    r = rr;
+    if (Ph::kClampU) {
+        const uint32_t mu = max(max(fbits(u.x) & 0x7fffffffu, fbits(u.y) & 0x7fffffffu),
+                                max(fbits(v.x) & 0x7fffffffu, fbits(v.y) & 0x7fffffffu));
+        const uint32_t mr = max(fbits(r.x), fbits(r.y));
+        if (mu > fbits(0.4f) || mr > fbits(1.5f)) {
+            u.x = fminf(0.4f, fmaxf(-0.4f, u.x));
+            u.y = fminf(0.4f, fmaxf(-0.4f, u.y));
+            v.x = fminf(0.4f, fmaxf(-0.4f, v.x));
+            v.y = fminf(0.4f, fmaxf(-0.4f, v.y));
+            r.x = fminf(1.5f, fmaxf(0.0f, r.x));
+            r.y = fminf(1.5f, fmaxf(0.0f, r.y));
+        }
+    }
+    const float2 uu = mul2(u, u), vv = mul2(v, v);
+    float2 s = bc2(k.s_nu);
+    if (Ph::kSmag) {
+        // smag_rate
+        const float2 n7 = sub2(sub2(add2(sub2(f[1], f[2]), f[3]), f[4]), mul2(r, sub2(uu, vv)));
+        const float2 n8 = sub2(sub2(add2(sub2(f[5], f[6]), f[7]), f[8]), mul2(mul2(r, u), v));
+        const float2 q2 = add2(fma2(n7, n7, mul2(n8, n8)), bc2(1e-8f));
+        const float2 cq = mul2(bc2(k.cs2x18), make_float2(sqrtf(q2.x), sqrtf(q2.y)));
+        const float2 X = add2(bc2(k.tau0 * k.tau0), make_float2(cq.x / r.x, cq.y / r.y));
+        const float2 te = mul2(bc2(0.5f), add2(bc2(k.tau0), make_float2(sqrtf(X.x), sqrtf(X.y))));
+        s = make_float2(1.0f / te.x, 1.0f / te.y);
+    }
+    if (Ph::kMrt) {
+        // mrt_relax
+        const float2 f14 = add2(add2(add2(f[1], f[2]), f[3]), f[4]);
+        const float2 f58 = add2(add2(add2(f[5], f[6]), f[7]), f[8]);
+        float2 m1 = sub2(fma2(bc2(-4.0f), f[0], mul2(bc2(2.0f), f58)), f14);
+        float2 m2 = sub2(fma2(bc2(4.0f), f[0], f58), mul2(bc2(2.0f), f14));
+        const float2 m3 = mul2(r, u);
+        float2 m4 = add2(sub2(sub2(fma2(bc2(-2.0f), sub2(f[1], f[3]), f[5]), f[6]), f[7]), f[8]);
+        const float2 m5 = mul2(r, v);
+        float2 m6 = sub2(sub2(add2(fma2(bc2(-2.0f), sub2(f[2], f[4]), f[5]), f[6]), f[7]), f[8]);
+        float2 m7 = sub2(add2(sub2(f[1], f[2]), f[3]), f[4]);
+        float2 m8 = sub2(add2(sub2(f[5], f[6]), f[7]), f[8]);
+        const float2 usq = add2(uu, vv);
+        m1 = sub2(m1, mul2(bc2(k.s_e), sub2(m1, mul2(fma2(bc2(3.0f), usq, bc2(-2.0f)), r))));
+        m2 = sub2(m2, mul2(bc2(k.s_eps), sub2(m2, mul2(fma2(bc2(-3.0f), usq, bc2(1.0f)), r))));
+        m4 = sub2(m4, mul2(bc2(k.s_q), add2(m4, m3)));
+        m6 = sub2(m6, mul2(bc2(k.s_q), add2(m6, m5)));
+        m7 = sub2(m7, mul2(s, sub2(m7, mul2(r, sub2(uu, vv)))));
+        m8 = sub2(m8, mul2(s, sub2(m8, mul2(mul2(r, u), v))));
+        const float2 inv9 = bc2(0.1111111111f), inv36 = bc2(0.02777777778f);
+        const float2 t0 = add2(sub2(r, m1), m2);
+        const float2 t1 = sub2(sub2(mul2(bc2(4.0f), r), m1), mul2(bc2(2.0f), m2));
+        const float2 t2 = add2(fma2(bc2(4.0f), r, mul2(bc2(2.0f), m1)), m2);
+        const float2 a3 = mul2(bc2(6.0f), m3), a4 = mul2(bc2(6.0f), m4), a5 = mul2(bc2(6.0f), m5),
+                     a6 = mul2(bc2(6.0f), m6), a7 = mul2(bc2(9.0f), m7), a8 = mul2(bc2(9.0f), m8);
+        const float2 b4 = mul2(bc2(3.0f), m4), b6 = mul2(bc2(3.0f), m6);
+        f[0] = mul2(t0, inv9);
+        f[1] = mul2(add2(sub2(add2(t1, a3), a4), a7), inv36);
+        f[2] = mul2(sub2(sub2(add2(t1, a5), a6), a7), inv36);
+        f[3] = mul2(add2(add2(sub2(t1, a3), a4), a7), inv36);
+        f[4] = mul2(sub2(add2(sub2(t1, a5), a6), a7), inv36);
+        f[5] = mul2(add2(add2(add2(add2(add2(t2, a3), b4), a5), b6), a8), inv36);
+        f[6] = mul2(sub2(add2(add2(sub2(sub2(t2, a3), b4), a5), b6), a8), inv36);
+        f[7] = mul2(add2(sub2(sub2(sub2(sub2(t2, a3), b4), a5), b6), a8), inv36);
+        f[8] = mul2(sub2(sub2(sub2(add2(add2(t2, a3), b4), a5), b6), a8), inv36);
+    } else {
+        // bgk_relax
+        const float2 usq = add2(uu, vv);
+#pragma unroll
+        for (int q = 0; q < 9; ++q) {
+            const float2 cu = add2(mul2(bc2((float)cx(q)), u), mul2(bc2((float)cy(q)), v));
+            const float2 poly =
+                sub2(add2(add2(bc2(1.0f), mul2(bc2(3.0f), cu)), mul2(mul2(bc2(4.5f), cu), cu)), mul2(bc2(1.5f), usq));
+            const float2 feq = mul2(mul2(bc2(wgt(q)), r), poly);
+            f[q] = fma2(s, sub2(feq, f[q]), f[q]);
+        }
+    }
+    if (Ph::kClampF) {
+        uint32_t m3[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+            const float a = (3 * j) % 2 ? f[(3 * j) / 2].y : f[(3 * j) / 2].x;
+            const float b = (3 * j + 1) % 2 ? f[(3 * j + 1) / 2].y : f[(3 * j + 1) / 2].x;
+            const float c = (3 * j + 2) % 2 ? f[(3 * j + 2) / 2].y : f[(3 * j + 2) / 2].x;
+            m3[j] = __vimax3_u32(fbits(a), fbits(b), fbits(c));
+        }
+        const uint32_t mx = max(__vimax3_u32(m3[0], m3[1], m3[2]), __vimax3_u32(m3[3], m3[4], m3[5]));
+        if (mx > fbits(10.0f)) {
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                f[q].x = fminf(10.0f, fmaxf(0.0f, f[q].x));
+                f[q].y = fminf(10.0f, fmaxf(0.0f, f[q].y));
+            }
+        }
+    }
+}
+
 } // namespace lbm

@@ -67,8 +67,10 @@ struct RwCfg {
     static constexpr int CW = 64 - 2 * PADL;
     static constexpr int MODE = MODE_;
     static constexpr bool LID = LID_;
-    // two-cell collision on the packed FP32x2 pipe (collide_pair) or scalar (collide_multi)
-    static constexpr bool PACKED = PACKED_ && !Ph_::kRefOrder;
+    // two-cell collision on the packed FP32x2 pipe (collide_pair; collide_ref_pair for
+    // the reference's evaluation order, up to T = 3 only: its moment vector costs
+    // registers the deeper kernels do not have) or scalar (collide_multi, collide_bf)
+    static constexpr bool PACKED = PACKED_ && (!Ph_::kRefOrder || T_ <= 3);
     using Ph = Ph_;
     using St = St_;
     using E = typename St::T;
@@ -324,7 +326,10 @@ __device__ __forceinline__ void collide_two(float2 (&g)[9], const Phys &k, float
     if constexpr (C::MLP) {
         collide_pair_mlp<Ph, false>(g, false, false, 0.0f, k, mc.F, mc.stage, mc.zbuf, mc.lane, r, u, v);
     } else if constexpr (C::PACKED) {
-        collide_pair<Ph>(g, k, r, u, v);
+        if constexpr (Ph::kRefOrder)
+            collide_ref_pair<Ph>(g, k, r, u, v);
+        else
+            collide_pair<Ph>(g, k, r, u, v);
     } else {
         float f[2][9], r_[2], u_[2], v_[2];
 #pragma unroll

