@@ -86,7 +86,9 @@ class Solver:
     def run(self, f_a, f_b, mask, n_steps: int, T: int = 2, ux=None, uy=None, rho=None, stream=None) -> int:
         """n_steps steps fused T per launch; returns 1 when the result is in f_b.  The
         default T = 2 is the fastest depth measured on a B200 for domains larger
-        than the L2 cache (the register wavefront)."""
+        than the L2 cache (the register wavefront; T = 3 is close).  Domains periodic
+        in x advance one step per launch whatever T (the faster kernel there; the
+        slab layer runs them on the register wavefront with halo columns)."""
         from . import _ptr, _stream
 
         out = C.c_int(0)
