@@ -1,4 +1,5 @@
-// Register wavefront kernel: T fused pull steps (T even, 2..6) with the
+// Register wavefront kernel: T fused pull steps (1 <= T <= 6; the general
+// solver uses it for 2 <= T <= 6, the learned closure for 1 <= T <= 4) with the
 // intermediate time levels held in registers.
 //
 // Same state convention, boundary rules and per-cell codes as the shared-
