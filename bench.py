@@ -353,13 +353,14 @@ def main():
     # (lbm_visualize, scale 50) and the RGBA frame read back to pinned host
     # memory; the solid mask is the step's input, uploaded from pinned host
     # memory every frame.  The populations stay resident, as in the driver.
-    # Uploads, frames and read-backs run on three streams with two mask and two
-    # image buffers, so frame i+1 computes while frame i's image is copied out.
+    # Uploads, frames and colour map + read-backs run on three streams with two
+    # mask, macro and image buffers, so frame i+1 computes while frame i's image is
+    # drawn and copied out.
     host_m = [torch.from_numpy(mask_np).pin_memory() for _ in range(2)]
     dev_m = [torch.empty_like(mask) for _ in range(2)]
     host_img = [torch.empty((H, W, 4), dtype=torch.uint8).pin_memory() for _ in range(2)]
     dev_img = [torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda") for _ in range(2)]
-    dev_mac = [torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in range(3)]
+    dev_mac = [[torch.empty((H, W), dtype=torch.float32, device="cuda") for _ in range(3)] for _ in range(2)]
     up, down = torch.cuda.Stream(), torch.cuda.Stream()
     ev_up = [torch.cuda.Event() for _ in range(2)]
     ev_comp = [torch.cuda.Event() for _ in range(2)]
@@ -371,23 +372,23 @@ def main():
     def e2e_step(i):
         j = i & 1
         with torch.cuda.stream(up):
-            up.wait_event(ev_comp[j])  # frame i-2 has finished reading this mask buffer
+            up.wait_event(ev_down[j])  # frame i-2's colour map has finished reading this mask buffer
             dev_m[j].copy_(host_m[j], non_blocking=True)
             ev_up[j].record(up)
         stream.wait_event(ev_up[j])
-        stream.wait_event(ev_down[j])  # frame i-2's image has been copied out
+        stream.wait_event(ev_down[j])  # frame i-2's u, v, rho and image are done with
+        mac = dev_mac[j]
         for li in range(0 if args.inplace else n_launch):
             last = li == n_launch - 1
-            which = S.run(st["a"], st["b"], dev_m[j], T, T, *(dev_mac if last else (None, None, None)),
-                          stream=stream)
+            which = S.run(st["a"], st["b"], dev_m[j], T, T, *(mac if last else (None, None, None)), stream=stream)
             if which:
                 st["a"], st["b"] = st["b"], st["a"]
         if args.inplace:
-            S.run_inplace(st["a"], dev_m[j], args.frame, *dev_mac, stream=stream)
-        L.visualize(*dev_mac, dev_img[j], dev_m[j], W, H, 50.0, stream=stream)
+            S.run_inplace(st["a"], dev_m[j], args.frame, *mac, stream=stream)
         ev_comp[j].record(stream)
-        with torch.cuda.stream(down):
+        with torch.cuda.stream(down):  # colour map and read-back overlap the next frame's steps
             down.wait_event(ev_comp[j])
+            L.visualize(*mac, dev_img[j], dev_m[j], W, H, 50.0, stream=down)
             host_img[j].copy_(dev_img[j], non_blocking=True)
             ev_down[j].record(down)
 
