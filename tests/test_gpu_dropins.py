@@ -98,6 +98,30 @@ def test_core4_vs_reference_kernel_driver_size(W, H):
         assert rel_l2(host(g), host(r)) < REL_TOL
 
 
+@pytest.mark.parametrize("W,H", [(2048, 512), (4096, 1024)])
+def test_core4_run_vs_reference_kernel_driver_size(W, H):
+    """lbm_core4_run at T = 2 (the register wavefront with the packed two-cell
+    collision in the reference's evaluation order) against the reference kernel
+    stepped 50 times, at the drivers' size and the cylinder channel's."""
+    lib = ref_lib("libref_core4.so")
+    if lib is None:
+        pytest.skip("oracle/_ref not built")
+    mask, f0 = _driver_case(W, H)
+    m = dev(mask)
+    a, b = dev(f0), dev(f0)
+    ra, rb = dev(f0), dev(f0)
+    mac = [zeros(H, W) for _ in range(3)]
+    rmac = [zeros(H, W) for _ in range(3)]
+    which = L.core4_run(m, a, b, *mac, W, H, 1.8, 0.1, 50, 2)
+    for _ in range(50):
+        assert lib.ref_core4_step(ptr(m), ptr(ra), ptr(rb), *[ptr(t) for t in rmac], W, H, 1.8, 0.1, 1.8,
+                                  stream()) == 0
+        ra, rb = rb, ra
+    assert rel_l2(host(b if which else a), host(ra)) < REL_TOL
+    for g, r in zip(mac, rmac):
+        assert rel_l2(host(g), host(r)) < REL_TOL
+
+
 @pytest.mark.parametrize("W,H", SIZES)
 def test_smemaa_vs_oracle(W, H):
     mask, f0 = _case(W, H, 3)
